@@ -1,0 +1,457 @@
+#!/usr/bin/env python
+"""Benchmark: 30-qubit complex128 gate application on one B200.
+
+Workload (one "step"): the 30-qubit brickwork circuit of depth 40 (per layer a U3 on every
+qubit with seeded angles, then CX on a seeded random perfect matching; 1800 gates) applied
+with the engine's fusion pass to a device-resident 2^30-amplitude state (16 GiB, far larger
+than the 126 MB L2, so no L2 flush is needed between steps).
+
+Metric: gate-apply GB/s = algorithmic bytes of the source gates (32 * 2^n * f per gate,
+f = fraction of amplitudes the gate can change) / device time.  Also reported: the
+per-target single-gate sweep (one U3 on each target 0..29), QFT(30) on a random state,
+batched adjoint gradients/s against the plain one-set-at-a-time GPU path, and the
+reference's OpenMP CPU path timed on this host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "30q gate-apply GB/s vs HBM peak; batched adjoint grads/s vs plain GPU path"
+UNIT = "GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=40)
+    ap.add_argument("--seed", type=int, default=2025)
+    ap.add_argument("--fusion-width", type=int, default=0)
+    ap.add_argument("--fusion-mode", type=int, default=0)
+    ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_arm(args):
+    """The reference's own OpenMP CPU implementation (oracle/_ref) on this host's cores,
+    on a bounded sample of the same workload: each step applies the first G gates of the
+    30-qubit brickwork circuit to a 16 GiB host state (G sized so a step takes ~3 s)."""
+    from oracle.oracle import Ref
+    import litequantumcomputingsimulator_b200 as lq
+    from litequantumcomputingsimulator_b200 import workloads as W
+    if not Ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liblqcs_ref.so was not built"}))
+        return 0
+    ref = Ref()
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    n = args.qubits
+    qc = W.brickwork(n, args.depth, args.seed)
+    insts = qc.instructions()
+    # size the sample: time one gate first
+    one = lq.QuantumCircuit(n)
+    one.append(insts[0])
+    try:
+        t1 = ref.time_apply(one, 1)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference could not run: {e}"}))
+        return 0
+    g = max(1, min(len(insts), int(3.0 / max(t1, 1e-3))))
+    sample = lq.QuantumCircuit(n)
+    for inst in insts[:g]:
+        sample.append(inst)
+    nbytes = W.alg_bytes(sample)
+    for _ in range(args.warmup):
+        ref.time_apply(sample, 1)
+    times = [ref.time_apply(sample, 1) for _ in range(args.steps)]
+    total = sum(times)
+    value = nbytes * args.steps / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded brickwork)",
+        "config": {"workload": f"brickwork n={n} depth={args.depth} seed={args.seed}",
+                   "sample": f"first {g} of {len(insts)} gates per step", "l2": "state > L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"first {g} gates of the {n}-qubit brickwork circuit per step, "
+                                   "OpenMP kernels of the reference on a pre-touched host state"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ CPU baseline leg
+def cpu_baseline(n: int, qc, budget_s: float = 12.0) -> dict:
+    from oracle.oracle import Ref, Port
+    import litequantumcomputingsimulator_b200 as lq
+    from litequantumcomputingsimulator_b200 import workloads as W
+    insts = qc.instructions()
+    if Ref.available():
+        ref = Ref()
+        cores = os.cpu_count() or 1
+        ref.set_threads(cores)
+        one = lq.QuantumCircuit(n)
+        one.append(insts[0])
+        t1 = ref.time_apply(one, 1)
+        g = max(1, min(len(insts), int(budget_s / max(t1, 1e-3))))
+        sample = lq.QuantumCircuit(n)
+        for inst in insts[:g]:
+            sample.append(inst)
+        t = ref.time_apply(sample, 1)
+        return {"value": W.alg_bytes(sample) / t / 1e9, "unit": UNIT, "cores": cores,
+                "kind": "reference",
+                "sample": f"first {g} gates of the {n}-qubit brickwork, reference OpenMP kernels, "
+                          f"{t:.2f} s"}
+    # the scalar port on a 26-qubit sample, one core
+    m = min(n, 26)
+    port = Port()
+    st = np.zeros(1 << m, dtype=np.complex128)
+    st[0] = 1
+    small = W.brickwork(m, 1, 7)
+    t0 = time.perf_counter()
+    k = 0
+    for inst in small.instructions():
+        port.apply_instruction(st, inst)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    sub = lq.QuantumCircuit(m)
+    for inst in small.instructions()[:k]:
+        sub.append(inst)
+    return {"value": W.alg_bytes(sub) / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {k} gates of a {m}-qubit brickwork layer, scalar C restatement"}
+
+
+# ------------------------------------------------------------------ engine arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        return reference_arm(args)
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import litequantumcomputingsimulator_b200 as lq
+    from litequantumcomputingsimulator_b200 import _native as N
+    from litequantumcomputingsimulator_b200 import workloads as W
+
+    n, depth = args.qubits, args.depth
+    qc = W.brickwork(n, depth, args.seed)
+    gate_bytes = W.alg_bytes(qc)
+    n_gates = qc.num_instructions()
+    hbm_peak, peak_kind = peaks()
+
+    prog = lq.simulator.CompiledCircuit(qc, True, args.fusion_width, args.fusion_mode)
+    sv = lq.Statevector(n)   # |0...0>, device resident
+
+    def step():
+        prog.apply(sv)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(dist)
+    launches0 = N.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(args.steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    launches = N.launch_count() - launches0
+    ms = start.elapsed_time(stop)
+    ms = max_over_ranks(ms, dist, device)
+    barrier(dist)
+    ms_per_step = ms / args.steps
+    value = gate_bytes * args.steps * world / (ms / 1e3) / 1e9
+
+    # ---- roofline of the dominant kernel: one profiled application (CUDA events per op)
+    prof = prog.profile(sv)
+    by_kernel = {}
+    for r in prof:
+        k = by_kernel.setdefault(r["kernel"], {"ms": 0.0, "bytes": 0.0, "launches": 0})
+        k["ms"] += r["ms"]
+        k["bytes"] += r["alg_bytes"]
+        k["launches"] += 1
+    dom_name, dom = max(by_kernel.items(), key=lambda kv: kv[1]["ms"])
+    prof_total = sum(v["ms"] for v in by_kernel.values())
+    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                "traffic": None, "launches": dom["launches"],
+                "share": dom["ms"] / prof_total,
+                "alg_bytes_per_launch": dom["bytes"] / dom["launches"],
+                "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                                "share": round(v["ms"] / prof_total, 4),
+                                "gbs": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1)}
+                            for k, v in by_kernel.items()}}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras = run_extras(lq, W, N, n, sv, hbm_peak, args)
+
+    # ---- e2e through the public API: run_statevector + D2H of the final state
+    e2e = None
+    if rank == 0:
+        e2e = run_e2e(lq, qc, gate_bytes, args)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and world == 1:
+        try:
+            cpu = cpu_baseline(n, qc)
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded brickwork circuit, random-init |0> state)",
+            "config": {"workload": f"brickwork n={n} depth={depth} seed={args.seed} "
+                                   f"({n_gates} gates), fused ({prog.n_ops} device ops)",
+                       "qubits": n, "depth": depth, "gates": n_gates,
+                       "fusion_width": args.fusion_width or "default", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (16 GiB state)"},
+            "gpu_launches": launches,
+            "gates_per_s": n_gates * args.steps * world / (ms / 1e3),
+            "clocks": clock_info,
+            "roofline": roofline,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "extras": extras,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(lq, qc, gate_bytes, args):
+    import torch
+    n = qc.num_qubits()
+    try:
+        host = torch.empty(1 << n, dtype=torch.complex128, pin_memory=True).numpy()
+        pinned = True
+    except Exception:  # noqa: BLE001
+        host = np.empty(1 << n, dtype=np.complex128)
+        pinned = False
+    sim = lq.StatevectorSimulator(fuse_gates=True, max_fusion_width=args.fusion_width,
+                                  fusion_mode=args.fusion_mode)
+    arr, cnt, _k = qc.c_instructions()
+    h2d = cnt * 80 + sum(len(i.gate.mat) * 16 for i in qc.instructions())
+    reps = max(1, min(args.steps, 2))
+    sv = sim.run_statevector(qc)
+    sv.to_numpy(out=host)
+    del sv
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sv = sim.run_statevector(qc)
+        sv.to_numpy(out=host)
+        del sv
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": gate_bytes / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(16 << n), "s_per_step": dt, "pinned": pinned,
+            "path": "StatevectorSimulator.run_statevector + Statevector.to_numpy (D2H)"}
+
+
+def run_extras(lq, W, N, n, sv, hbm_peak, args):
+    import torch
+    out = {}
+    # per-target sweep: one U3 on target t, timed over R launches
+    sweep = {}
+    reps = 5
+    for t in range(n):
+        c = lq.QuantumCircuit(n)
+        c.u(0.3, 0.5, 0.7, t)
+        p = lq.simulator.CompiledCircuit(c, fuse_gates=False)
+        p.apply(sv)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            p.apply(sv)
+        e.record()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / reps
+        sweep[t] = 32.0 * (1 << n) / (ms / 1e3) / 1e9
+    vals = list(sweep.values())
+    out["per_target_u3_gbs"] = {str(k): round(v, 1) for k, v in sweep.items()}
+    out["per_target_u3_min_frac"] = min(vals) / hbm_peak
+    out["per_target_u3_median_frac"] = statistics.median(vals) / hbm_peak
+
+    # unfused gate-by-gate path on the same brickwork (for the fusion speed-up)
+    qc = W.brickwork(n, args.depth, args.seed)
+    plain = lq.simulator.CompiledCircuit(qc, fuse_gates=False)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    plain.apply(sv)
+    e.record()
+    torch.cuda.synchronize()
+    ms_plain = s.elapsed_time(e)
+    out["brickwork_unfused_gbs"] = W.alg_bytes(qc) / (ms_plain / 1e3) / 1e9
+    out["brickwork_unfused_ms"] = ms_plain
+
+    # QFT(n) on a random state: the state is filled on the device side by a random circuit
+    # would change the workload; instead the Gaussian state is uploaded once (not timed)
+    try:
+        qft = lq.algorithms.qft(n)
+        pq = lq.simulator.CompiledCircuit(qft, fuse_gates=True)
+        pq.apply(sv)
+        torch.cuda.synchronize()
+        s.record()
+        pq.apply(sv)
+        e.record()
+        torch.cuda.synchronize()
+        ms_q = s.elapsed_time(e)
+        out["qft_ms"] = ms_q
+        out["qft_gates"] = qft.num_instructions()
+        out["qft_gbs"] = W.alg_bytes(qft) / (ms_q / 1e3) / 1e9
+        out["qft_device_ops"] = pq.n_ops
+    except Exception as ex:  # noqa: BLE001
+        out["qft_error"] = str(ex)
+
+    # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets)
+    try:
+        pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+        ham = W.random_hamiltonian(16, 500, seed=12)
+        sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
+        lq.algorithms.adjoint_gradient(ham, pc, sets[:8], max_resident=8)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lq.algorithms.adjoint_gradient(ham, pc, sets, max_resident=64)
+        t_b = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for b in range(16):
+            lq.algorithms.adjoint_gradient(ham, pc, sets[b], max_resident=1)
+        t_p = (time.perf_counter() - t0) / 16
+        out["adjoint_batched_grads_per_s"] = 256 / t_b
+        out["adjoint_plain_grads_per_s"] = 1 / t_p
+        out["adjoint_speedup_vs_plain"] = (256 / t_b) * t_p
+    except Exception as ex:  # noqa: BLE001
+        out["adjoint_error"] = str(ex)
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

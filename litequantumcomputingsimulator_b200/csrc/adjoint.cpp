@@ -1,0 +1,272 @@
+// adjoint.cpp — batched adjoint-state gradients of <psi(theta)|H|psi(theta)>.
+//
+// Engine extension: the reference differentiates by the parameter-shift rule, two full
+// circuit evaluations per parameter (algorithms::parameter_shift_gradient,
+// src/algorithms/vqe.cpp:68-94).  Every parameterised gate here is exp(-i theta/2 P) for a
+// Pauli string P (RX, RY, RZ, rp), so with psi_k the state after gate k and
+// lambda_k = U_{k+1}^dagger ... U_N^dagger H psi_N,
+//     dE/dtheta_k = 2 Re <lambda_k| (-i/2) P_k |psi_k> = Im <lambda_k| P_k |psi_k>.
+// One forward pass, one Hamiltonian application and one backward pass (undoing each gate
+// on psi and lambda) give all gradients.  Up to `max_resident` parameter sets advance
+// together: every kernel launch walks the whole resident batch (gridDim.y), the
+// parameterised rotations read one (cos, sin) per state.
+#include <algorithm>
+#include <cmath>
+
+#include "engine.hpp"
+
+namespace lqcs_b200 {
+
+void launch_batched_inner_re_p(const LaunchCtx& ctx, const double2* a, const double2* b,
+                               uint32_t n, uint32_t batch, double* d_partials, double* d_out);
+void launch_batched_pauli_im_p(const LaunchCtx& ctx, const double2* a, const double2* b,
+                               uint32_t n, uint32_t batch, uint64_t x, uint64_t zy,
+                               uint32_t n_y, double* d_partials, double* d_out,
+                               uint64_t out_stride);
+
+namespace {
+
+struct GateStep {
+    int param = -1;            // parameter index, -1 for a fixed gate
+    PauliMasks gen;            // generator of a parameterised gate (global masks)
+    Program fwd, inv;          // fixed gate and its inverse (one op each)
+};
+
+PauliMasks generator(const GateDesc& g) {
+    PauliMasks m;
+    const uint64_t t = uint64_t{1} << g.targets()[0];
+    switch (g.type) {
+        case LQCS_GATE_RX: m.x = t; break;
+        case LQCS_GATE_RY: m.x = t; m.zy = t; m.n_y = 1; break;
+        case LQCS_GATE_RZ: m.zy = t; break;
+        default: {
+            const PauliMasks loc = pauli_local_masks(g.pauli);
+            for (uint32_t j = 0; j < g.pauli.size(); ++j) {
+                if ((loc.x >> j) & 1) m.x |= uint64_t{1} << g.targets()[j];
+                if ((loc.zy >> j) & 1) m.zy |= uint64_t{1} << g.targets()[j];
+            }
+            m.n_y = loc.n_y;
+        }
+    }
+    return m;
+}
+
+// Inverse of one device op (conjugate transpose, inverse permutation).
+DevOp invert(const DevOp& op) {
+    DevOp r = op;
+    switch (op.kind) {
+        case OpKind::K1Q:
+            r.m1 = {std::conj(op.m1[0]), std::conj(op.m1[2]), std::conj(op.m1[1]),
+                    std::conj(op.m1[3])};
+            break;
+        case OpKind::PHASE:
+            r.phase = std::conj(op.phase);
+            break;
+        case OpKind::DIAG:
+            for (cd& z : r.mat) z = std::conj(z);
+            break;
+        case OpKind::DENSE: {
+            const uint64_t dim = uint64_t{1} << op.k;
+            for (uint64_t i = 0; i < dim; ++i)
+                for (uint64_t j = 0; j < dim; ++j) r.mat[j * dim + i] = std::conj(op.mat[i * dim + j]);
+            break;
+        }
+        case OpKind::PERM: {
+            // reverse every cycle
+            size_t s = 0;
+            for (uint32_t len : op.cycle_len) {
+                std::reverse(r.cycles.begin() + s, r.cycles.begin() + s + len);
+                s += len;
+            }
+            break;
+        }
+        case OpKind::PAULI:
+            r.sin_h = -op.sin_h;
+            break;
+    }
+    return r;
+}
+
+uint32_t default_resident(uint32_t n, uint64_t batch) {
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const uint64_t per_set = 2 * (uint64_t{16} << n);
+    const uint64_t fit = std::max<uint64_t>(1, (free_b / 2) / per_set);
+    return static_cast<uint32_t>(std::min<uint64_t>({batch, fit, 256}));
+}
+
+}  // namespace
+
+void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
+                     const double* params, uint64_t batch, uint32_t max_resident,
+                     double* energy_out, double* grad_out) {
+    std::vector<GateDesc> tmpl;
+    std::vector<uint64_t> pinst;
+    check_pc(pc, tmpl, pinst);
+    if (batch == 0) return;
+    if (!params && !pinst.empty()) invalid("adjoint_gradient: params is null");
+    const uint32_t n = pc->n_qubits;
+    const uint64_t np = pinst.size();
+    const uint64_t len = uint64_t{1} << n;
+
+    std::vector<int> param_of(tmpl.size(), -1);
+    for (uint64_t p = 0; p < np; ++p) param_of[pinst[p]] = static_cast<int>(p);
+
+    // States smaller than one lane chunk use the per-set dense path: bind and evolve.
+    if (n < 5) {
+        auto st = new_state(n, 1, nullptr);
+        auto lam = new_state(n, 1, nullptr);
+        FusionConfig none;
+        none.fuse = false;
+        DeviceBuffer d_terms, part, d_out;
+        for (uint64_t b = 0; b < batch; ++b) {
+            const double* th = params + b * np;
+            std::vector<GateDesc> bound = bind_params(tmpl, pinst, th);
+            launch_set_basis(st->ctx, st->d(), n, 1, 0);
+            apply_circuit(*st, bound, none);
+            // lambda = H psi
+            std::vector<PauliTermDev> terms;
+            static const cd ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+            for (size_t t = 0; t < h.terms.size(); ++t) {
+                const cd c = h.coeffs[t] * ipow[h.terms[t].n_y % 4];
+                terms.push_back({h.terms[t].x, h.terms[t].zy, make_double2(c.real(), c.imag())});
+            }
+            d_terms.ensure(sizeof(PauliTermDev) * std::max<size_t>(1, terms.size()));
+            if (!terms.empty())
+                cuda_check(cudaMemcpy(d_terms.ptr, terms.data(), sizeof(PauliTermDev) * terms.size(),
+                                      cudaMemcpyHostToDevice), "H2D terms");
+            if (terms.empty()) cuda_check(cudaMemset(lam->d(), 0, sizeof(double2) * len), "memset");
+            else launch_apply_hamiltonian(st->ctx, st->d(), lam->d(), n, 1,
+                                          d_terms.as<PauliTermDev>(), static_cast<uint32_t>(terms.size()));
+            part.ensure(sizeof(double) * 128);
+            d_out.ensure(sizeof(double) * (np + 1));
+            launch_batched_inner_re_p(st->ctx, st->d(), lam->d(), n, 1, part.as<double>(),
+                                      d_out.as<double>() + np);
+            for (size_t i = tmpl.size(); i-- > 0;) {
+                const GateDesc& g = bound[i];
+                if (!g.is_unitary()) continue;
+                if (param_of[i] >= 0) {
+                    const PauliMasks m = generator(g);
+                    launch_batched_pauli_im_p(st->ctx, lam->d(), st->d(), n, 1, m.x, m.zy, m.n_y,
+                                              part.as<double>(), d_out.as<double>() + param_of[i], 1);
+                }
+                Program inv;
+                std::vector<DevOp> ops{invert(lower_gate(g, n))};
+                inv.build(std::move(ops), nullptr);
+                inv.launch(st->ctx, st->d(), n, 1);
+                inv.launch(st->ctx, lam->d(), n, 1);
+            }
+            std::vector<double> out(np + 1);
+            cuda_check(cudaMemcpy(out.data(), d_out.ptr, sizeof(double) * (np + 1),
+                                  cudaMemcpyDeviceToHost), "D2H gradients");
+            if (energy_out) energy_out[b] = out[np];
+            if (grad_out) std::copy(out.begin(), out.begin() + np, grad_out + b * np);
+        }
+        return;
+    }
+
+    // Precompile the fixed gates (and their inverses); barrier/measure are skipped.
+    std::vector<GateStep> steps;
+    steps.reserve(tmpl.size());
+    for (size_t i = 0; i < tmpl.size(); ++i) {
+        const GateDesc& g = tmpl[i];
+        if (g.type == LQCS_GATE_RESET) invalid("run_statevector: Reset is non-deterministic; use run() instead");
+        if (!g.is_unitary()) continue;
+        GateStep s;
+        s.param = param_of[i];
+        if (s.param >= 0) {
+            s.gen = generator(g);
+        } else {
+            const DevOp op = lower_gate(g, n);
+            s.fwd.build({op}, nullptr);
+            s.inv.build({invert(op)}, nullptr);
+        }
+        steps.push_back(std::move(s));
+    }
+
+    const uint32_t R = max_resident ? static_cast<uint32_t>(std::min<uint64_t>(max_resident, batch))
+                                    : default_resident(n, batch);
+    auto psi = new_state(n, R, nullptr);
+    auto lam = new_state(n, R, nullptr);
+    const LaunchCtx ctx = psi->ctx;
+
+    std::vector<PauliTermDev> terms;
+    static const cd ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+    for (size_t t = 0; t < h.terms.size(); ++t) {
+        const cd c = h.coeffs[t] * ipow[h.terms[t].n_y % 4];
+        terms.push_back({h.terms[t].x, h.terms[t].zy, make_double2(c.real(), c.imag())});
+    }
+    DeviceBuffer d_terms, d_cs, d_csi, d_part, d_energy, d_grad;
+    d_terms.ensure(sizeof(PauliTermDev) * std::max<size_t>(1, terms.size()));
+    if (!terms.empty())
+        cuda_check(cudaMemcpy(d_terms.ptr, terms.data(), sizeof(PauliTermDev) * terms.size(),
+                              cudaMemcpyHostToDevice), "H2D terms");
+    d_cs.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
+    d_csi.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
+    d_part.ensure(sizeof(double) * 64 * R);
+    d_energy.ensure(sizeof(double) * R);
+    d_grad.ensure(sizeof(double) * std::max<uint64_t>(1, np) * R);
+    std::vector<double2> cs(np * R), csi(np * R);
+    std::vector<double> h_energy(R), h_grad(np * R);
+
+    for (uint64_t b0 = 0; b0 < batch; b0 += R) {
+        const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(R, batch - b0));
+        // (cos, sin) of theta/2 per parameter and set; layout [param][set]
+        for (uint64_t p = 0; p < np; ++p) {
+            for (uint32_t b = 0; b < nb; ++b) {
+                const double hh = params[(b0 + b) * np + p] / 2;
+                cs[p * R + b] = make_double2(std::cos(hh), std::sin(hh));
+                csi[p * R + b] = make_double2(std::cos(hh), -std::sin(hh));
+            }
+        }
+        if (np) {
+            cuda_check(cudaMemcpy(d_cs.ptr, cs.data(), sizeof(double2) * np * R, cudaMemcpyHostToDevice), "H2D");
+            cuda_check(cudaMemcpy(d_csi.ptr, csi.data(), sizeof(double2) * np * R, cudaMemcpyHostToDevice), "H2D");
+        }
+        launch_set_basis(ctx, psi->d(), n, nb, 0);
+        for (const GateStep& s : steps) {
+            if (s.param >= 0) {
+                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y,
+                                              d_cs.as<double2>() + static_cast<uint64_t>(s.param) * R);
+            } else {
+                s.fwd.launch(ctx, psi->d(), n, nb);
+            }
+        }
+        if (terms.empty()) {
+            cuda_check(cudaMemsetAsync(lam->d(), 0, sizeof(double2) * len * nb, ctx.stream), "memset");
+        } else {
+            launch_apply_hamiltonian(ctx, psi->d(), lam->d(), n, nb, d_terms.as<PauliTermDev>(),
+                                     static_cast<uint32_t>(terms.size()));
+        }
+        launch_batched_inner_re_p(ctx, psi->d(), lam->d(), n, nb, d_part.as<double>(),
+                                  d_energy.as<double>());
+        for (size_t i = steps.size(); i-- > 0;) {
+            const GateStep& s = steps[i];
+            if (s.param >= 0) {
+                launch_batched_pauli_im_p(ctx, lam->d(), psi->d(), n, nb, s.gen.x, s.gen.zy,
+                                          s.gen.n_y, d_part.as<double>(),
+                                          d_grad.as<double>() + s.param, np);
+                const double2* inv = d_csi.as<double2>() + static_cast<uint64_t>(s.param) * R;
+                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+                launch_pauli_rotation_batched(ctx, lam->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+            } else {
+                s.inv.launch(ctx, psi->d(), n, nb);
+                s.inv.launch(ctx, lam->d(), n, nb);
+            }
+        }
+        cuda_check(cudaMemcpyAsync(h_energy.data(), d_energy.ptr, sizeof(double) * nb,
+                                   cudaMemcpyDeviceToHost, ctx.stream), "D2H energies");
+        if (np)
+            cuda_check(cudaMemcpyAsync(h_grad.data(), d_grad.ptr, sizeof(double) * np * nb,
+                                       cudaMemcpyDeviceToHost, ctx.stream), "D2H gradients");
+        cuda_check(cudaStreamSynchronize(ctx.stream), "adjoint");
+        for (uint32_t b = 0; b < nb; ++b) {
+            if (energy_out) energy_out[b0 + b] = h_energy[b];
+            if (grad_out)
+                std::copy(h_grad.begin() + b * np, h_grad.begin() + (b + 1) * np,
+                          grad_out + (b0 + b) * np);
+        }
+    }
+}
+
+}  // namespace lqcs_b200

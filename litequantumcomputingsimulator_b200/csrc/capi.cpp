@@ -1,0 +1,415 @@
+// capi.cpp — the extern "C" boundary (include/lqcs_b200.h).  Every entry point runs its
+// body under `guarded`, which turns engine errors into status codes and keeps the message
+// for lqcs_last_error().
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "engine.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return LQCS_OK;
+    } catch (const lqcs_b200::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "out of host memory";
+        return LQCS_ERR_OUT_OF_MEMORY;
+    } catch (const std::logic_error& e) {
+        g_last_error = e.what();
+        return LQCS_ERR_LOGIC;
+    } catch (const std::runtime_error& e) {
+        g_last_error = e.what();
+        return LQCS_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return LQCS_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return LQCS_ERR_INTERNAL;
+    }
+}
+
+void need(const void* p, const char* what) {
+    if (p == nullptr) lqcs_b200::invalid(std::string(what) + " is null");
+}
+
+lqcs_b200::FusionConfig fusion_of(int32_t fuse, int32_t width, int32_t mode) {
+    lqcs_b200::FusionConfig fc;
+    fc.fuse = fuse != 0;
+    if (width < 0 || width > lqcs_b200::kMaxDense) lqcs_b200::invalid("fusion width must be in [1, 6]");
+    fc.max_width = static_cast<uint32_t>(width);
+    fc.mode = mode;
+    return fc;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lqcs_last_error(void) { return g_last_error.c_str(); }
+
+const char* lqcs_version(void) { return "lqcs_b200 0.1.0 sm_100a"; }
+
+uint64_t lqcs_kernel_launch_count(void) { return lqcs_b200::launch_count(); }
+
+int lqcs_state_create(uint32_t n_qubits, void* stream, lqcs_state** out) {
+    return guarded([&] {
+        need(out, "out");
+        auto st = lqcs_b200::new_state(n_qubits, 1, static_cast<cudaStream_t>(stream));
+        st->sync();
+        *out = st.release();
+    });
+}
+
+int lqcs_state_create_batch(uint32_t n_qubits, uint32_t batch, void* stream, lqcs_state** out) {
+    return guarded([&] {
+        need(out, "out");
+        auto st = lqcs_b200::new_state(n_qubits, batch, static_cast<cudaStream_t>(stream));
+        st->sync();
+        *out = st.release();
+    });
+}
+
+int lqcs_state_destroy(lqcs_state* st) {
+    return guarded([&] {
+        if (!st) return;
+        cudaStreamSynchronize(st->stream);
+        delete st;
+    });
+}
+
+int lqcs_state_num_qubits(const lqcs_state* st, uint32_t* out) {
+    return guarded([&] {
+        need(st, "state");
+        need(out, "out");
+        *out = st->n;
+    });
+}
+
+int lqcs_state_device_ptr(const lqcs_state* st, void** out) {
+    return guarded([&] {
+        need(st, "state");
+        need(out, "out");
+        *out = st->amps.ptr;
+    });
+}
+
+int lqcs_state_set_zero(lqcs_state* st) {
+    return guarded([&] {
+        need(st, "state");
+        lqcs_b200::launch_set_basis(st->ctx, st->d(), st->n, st->batch, 0);
+        st->sync();
+    });
+}
+
+int lqcs_state_load(lqcs_state* st, const double* host_amps, uint64_t n_amps) {
+    return guarded([&] {
+        need(st, "state");
+        need(host_amps, "host_amps");
+        if (n_amps != st->len() && n_amps != st->len() * st->batch)
+            lqcs_b200::invalid("state_load: amplitude count must be 2^n (or 2^n * batch)");
+        lqcs_b200::cuda_check(cudaMemcpyAsync(st->amps.ptr, host_amps, n_amps * sizeof(double2),
+                                              cudaMemcpyHostToDevice, st->stream),
+                              "H2D amplitudes");
+        st->sync();
+    });
+}
+
+int lqcs_state_store(const lqcs_state* st, double* host_amps, uint64_t n_amps) {
+    return guarded([&] {
+        need(st, "state");
+        need(host_amps, "host_amps");
+        if (n_amps != st->len() && n_amps != st->len() * st->batch)
+            lqcs_b200::invalid("state_store: amplitude count must be 2^n (or 2^n * batch)");
+        lqcs_b200::cuda_check(cudaMemcpyAsync(host_amps, st->amps.ptr, n_amps * sizeof(double2),
+                                              cudaMemcpyDeviceToHost, st->stream),
+                              "D2H amplitudes");
+        st->sync();
+    });
+}
+
+int lqcs_state_apply(lqcs_state* st, const lqcs_instruction* insts, uint64_t n_insts,
+                     int32_t fuse_gates, int32_t max_fusion_width, int32_t fusion_mode) {
+    return guarded([&] {
+        need(st, "state");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, st->n);
+        lqcs_b200::apply_circuit(*st, gates, fusion_of(fuse_gates, max_fusion_width, fusion_mode));
+    });
+}
+
+int lqcs_program_create(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                        int32_t fuse_gates, int32_t max_fusion_width, int32_t fusion_mode,
+                        lqcs_program** out) {
+    return guarded([&] {
+        need(out, "out");
+        if (n_qubits == 0) lqcs_b200::invalid("QuantumCircuit: num_qubits must be >= 1");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        *out = lqcs_b200::program_create(n_qubits, gates,
+                                         fusion_of(fuse_gates, max_fusion_width, fusion_mode))
+                   .release();
+    });
+}
+
+int lqcs_program_destroy(lqcs_program* prog) {
+    return guarded([&] { delete prog; });
+}
+
+int lqcs_program_info(const lqcs_program* prog, uint64_t* n_ops, uint64_t* n_gates) {
+    return guarded([&] {
+        need(prog, "program");
+        if (n_ops) *n_ops = prog->prog.ops.size();
+        if (n_gates) *n_gates = prog->prog.source_gates;
+    });
+}
+
+int lqcs_program_apply(lqcs_state* st, const lqcs_program* prog) {
+    return guarded([&] {
+        need(st, "state");
+        need(prog, "program");
+        if (prog->n != st->n) lqcs_b200::invalid("program_apply: qubit count mismatch");
+        prog->prog.launch(st->ctx, st->d(), st->n, st->batch);
+        st->sync();
+    });
+}
+
+int lqcs_program_apply_profiled(lqcs_state* st, const lqcs_program* prog, uint64_t cap,
+                                lqcs_op_profile* out, uint64_t* n_out) {
+    return guarded([&] {
+        need(st, "state");
+        need(prog, "program");
+        need(n_out, "n_out");
+        if (prog->n != st->n) lqcs_b200::invalid("program_apply: qubit count mismatch");
+        lqcs_b200::program_profile(*st, *prog, cap, out, n_out);
+    });
+}
+
+int lqcs_run_statevector(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                         const lqcs_sim_options* opts, void* stream, lqcs_state** out) {
+    return guarded([&] {
+        need(out, "out");
+        if (opts && opts->n_channels > 0) {
+            lqcs_b200::invalid(
+                "run_statevector: noisy simulation is stochastic (one trajectory is not the "
+                "quantum state); use run() or DensityMatrixSimulator");
+        }
+        if (n_qubits == 0) lqcs_b200::invalid("QuantumCircuit: num_qubits must be >= 1");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        auto st = lqcs_b200::new_state(n_qubits, 1, static_cast<cudaStream_t>(stream));
+        const int32_t fuse = opts ? opts->fuse_gates : 1;
+        const int32_t width = opts ? opts->max_fusion_width : 0;
+        const int32_t mode = opts ? opts->fusion_mode : 0;
+        lqcs_b200::apply_circuit(*st, gates, fusion_of(fuse, width, mode));
+        *out = st.release();
+    });
+}
+
+int lqcs_run(uint32_t n_qubits, uint32_t n_clbits, const lqcs_instruction* insts,
+             uint64_t n_insts, uint64_t shots, const lqcs_sim_options* opts,
+             uint64_t* shot_registers) {
+    return guarded([&] {
+        if (n_qubits == 0) lqcs_b200::invalid("QuantumCircuit: num_qubits must be >= 1");
+        if (shots > 0) need(shot_registers, "shot_registers");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        lqcs_b200::run_shots(n_qubits, n_clbits, gates, shots, opts, shot_registers);
+    });
+}
+
+int lqcs_state_read_range(const lqcs_state* st, uint64_t first, uint64_t count, double* host) {
+    return guarded([&] {
+        need(st, "state");
+        if (count == 0) return;
+        need(host, "host");
+        if (first >= st->len() * st->batch || count > st->len() * st->batch - first)
+            lqcs_b200::out_of_range("state_read_range: index out of range");
+        lqcs_b200::cuda_check(cudaMemcpyAsync(host, st->d() + first, count * sizeof(double2),
+                                              cudaMemcpyDeviceToHost, st->stream),
+                              "D2H amplitudes");
+        st->sync();
+    });
+}
+
+int lqcs_gate_matrix(const lqcs_instruction* inst, int32_t with_controls, double* out,
+                     uint64_t cap_doubles, uint64_t* dim_out) {
+    return guarded([&] {
+        need(inst, "instruction");
+        need(dim_out, "dim_out");
+        uint32_t max_q = 0;
+        for (uint32_t i = 0; i < inst->n_qubits; ++i) max_q = std::max(max_q, inst->qubits[i] + 1);
+        const lqcs_b200::GateDesc g = lqcs_b200::decode(*inst, std::max<uint32_t>(max_q, 1));
+        const std::vector<lqcs_b200::cd> m = with_controls ? g.full_matrix() : g.base_matrix();
+        uint64_t dim = 1;
+        while (dim * dim < m.size()) dim <<= 1;
+        *dim_out = dim;
+        if (out == nullptr) return;
+        if (cap_doubles < 2 * m.size()) lqcs_b200::invalid("gate_matrix: output buffer too small");
+        for (size_t i = 0; i < m.size(); ++i) {
+            out[2 * i] = m[i].real();
+            out[2 * i + 1] = m[i].imag();
+        }
+    });
+}
+
+int lqcs_state_probabilities(const lqcs_state* st, double* host_out) {
+    return guarded([&] {
+        need(st, "state");
+        need(host_out, "host_out");
+        lqcs_b200::DeviceBuffer p;
+        p.ensure(sizeof(double) * st->len());
+        lqcs_b200::launch_probabilities(st->ctx, st->d(), st->n, p.as<double>());
+        lqcs_b200::cuda_check(cudaMemcpyAsync(host_out, p.ptr, sizeof(double) * st->len(),
+                                              cudaMemcpyDeviceToHost, st->stream),
+                              "D2H probabilities");
+        st->sync();
+    });
+}
+
+int lqcs_state_norm(const lqcs_state* st, double* out) {
+    return guarded([&] {
+        need(st, "state");
+        need(out, "out");
+        *out = std::sqrt(lqcs_b200::state_norm2(*const_cast<lqcs_state*>(st)));
+    });
+}
+
+int lqcs_state_sample(const lqcs_state* st, const double* uniforms, uint64_t shots,
+                      uint64_t* idx_out, double* min_margin) {
+    return guarded([&] {
+        need(st, "state");
+        if (shots > 0) {
+            need(uniforms, "uniforms");
+            need(idx_out, "idx_out");
+        }
+        lqcs_b200::sample(*const_cast<lqcs_state*>(st), uniforms, shots, idx_out, min_margin);
+    });
+}
+
+int lqcs_state_expectation_pauli(const lqcs_state* st, const char* pauli, double* out) {
+    return guarded([&] {
+        need(st, "state");
+        need(out, "out");
+        const auto m = lqcs_b200::pauli_global_masks(pauli, st->n, "expectation_value");
+        *out = lqcs_b200::expectation_terms(*const_cast<lqcs_state*>(st), {m})[0];
+    });
+}
+
+int lqcs_state_expectation_terms(const lqcs_state* st, const char* const* paulis,
+                                 const double* coeffs, uint64_t n_terms, double* per_term,
+                                 double* total) {
+    return guarded([&] {
+        need(st, "state");
+        if (n_terms > 0) {
+            need(paulis, "paulis");
+            need(coeffs, "coeffs");
+        }
+        std::vector<lqcs_b200::PauliMasks> terms;
+        for (uint64_t t = 0; t < n_terms; ++t)
+            terms.push_back(lqcs_b200::pauli_global_masks(paulis[t], st->n, "expectation_value"));
+        const auto v = lqcs_b200::expectation_terms(*const_cast<lqcs_state*>(st), terms);
+        double e = 0.0;
+        for (uint64_t t = 0; t < n_terms; ++t) {
+            if (per_term) per_term[t] = v[t];
+            e += coeffs[t] * v[t];
+        }
+        if (total) *total = e;
+    });
+}
+
+int lqcs_state_collapse(lqcs_state* st, uint32_t qubit, double uniform, int32_t* outcome) {
+    return guarded([&] {
+        need(st, "state");
+        const int o = lqcs_b200::collapse(*st, qubit, uniform);
+        st->sync();
+        if (outcome) *outcome = o;
+    });
+}
+
+int lqcs_state_reset_qubit(lqcs_state* st, uint32_t qubit, double uniform) {
+    return guarded([&] {
+        need(st, "state");
+        if (qubit >= st->n) lqcs_b200::out_of_range("reset: qubit index out of range");
+        lqcs_b200::reset_qubit(*st, qubit, uniform);
+        st->sync();
+    });
+}
+
+int lqcs_state_kraus_probability(const lqcs_state* st, uint32_t qubit, const double* k,
+                                 double* out) {
+    return guarded([&] {
+        need(st, "state");
+        need(k, "k");
+        need(out, "out");
+        const std::array<lqcs_b200::cd, 4> kk{lqcs_b200::cd{k[0], k[1]}, lqcs_b200::cd{k[2], k[3]},
+                                              lqcs_b200::cd{k[4], k[5]}, lqcs_b200::cd{k[6], k[7]}};
+        *out = lqcs_b200::kraus_probability(*const_cast<lqcs_state*>(st), qubit, kk);
+    });
+}
+
+int lqcs_parameter_shift_gradient(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
+                                  const double* params, double* grad_out) {
+    return guarded([&] {
+        need(pc, "parametric circuit");
+        if (pc->n_params > 0) {
+            need(params, "params");
+            need(grad_out, "grad_out");
+        }
+        const auto ham = lqcs_b200::decode_hamiltonian(h, pc->n_qubits);
+        lqcs_b200::parameter_shift(pc, ham, params, grad_out);
+    });
+}
+
+int lqcs_adjoint_gradient(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
+                          const double* params, uint64_t batch, uint32_t max_resident,
+                          double* energy_out, double* grad_out) {
+    return guarded([&] {
+        need(pc, "parametric circuit");
+        const auto ham = lqcs_b200::decode_hamiltonian(h, pc->n_qubits);
+        lqcs_b200::adjoint_batched(pc, ham, params, batch, max_resident, energy_out, grad_out);
+    });
+}
+
+int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
+                        const double* params, uint64_t batch, uint32_t max_resident,
+                        double* energy_out) {
+    return guarded([&] {
+        need(pc, "parametric circuit");
+        need(energy_out, "energy_out");
+        const auto ham = lqcs_b200::decode_hamiltonian(h, pc->n_qubits);
+        lqcs_b200::adjoint_batched(pc, ham, params, batch, max_resident, energy_out, nullptr);
+    });
+}
+
+int lqcs_rng_uniforms(uint64_t seed, uint64_t count, double* out) {
+    return guarded([&] {
+        if (count > 0) need(out, "out");
+        lqcs_b200::Rng rng(seed);
+        for (uint64_t i = 0; i < count; ++i) out[i] = lqcs_b200::rng_uniform(rng);
+    });
+}
+
+int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                     int32_t max_fusion_width, int32_t fusion_mode, uint64_t cap,
+                     uint32_t* block_width, uint32_t* block_gates, uint64_t* n_blocks) {
+    return guarded([&] {
+        need(n_blocks, "n_blocks");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        const auto p = lqcs_b200::plan(gates, n_qubits, fusion_of(1, max_fusion_width, fusion_mode));
+        *n_blocks = p.size();
+        for (uint64_t i = 0; i < p.size() && i < cap; ++i) {
+            if (block_width) block_width[i] = static_cast<uint32_t>(p[i].qubits.size());
+            if (block_gates) block_gates[i] = static_cast<uint32_t>(p[i].gates.size());
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,761 @@
+// engine.cpp — device runtime: state handles, programs, run paths, expectations.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numbers>
+#include <optional>
+#include <string>
+
+namespace lqcs_b200 {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        throw Error(LQCS_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    throw Error(LQCS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void DeviceBuffer::ensure(size_t b) {
+    if (b <= bytes) return;
+    if (ptr) {
+        cuda_check(cudaFree(ptr), "cudaFree");
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cuda_check(cudaMalloc(&ptr, b), "cudaMalloc");
+    bytes = b;
+}
+
+int device_sm_count() {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+               "cudaDeviceGetAttribute");
+    cache[dev] = sms;
+    return sms;
+}
+
+LaunchCtx make_ctx(cudaStream_t s) {
+    LaunchCtx c;
+    c.stream = s;
+    c.num_sms = device_sm_count();
+    return c;
+}
+
+uint32_t default_fusion_width() {
+    if (const char* e = std::getenv("LQCS_FUSION_WIDTH")) {
+        const int v = std::atoi(e);
+        if (v >= 1 && v <= kMaxDense) return static_cast<uint32_t>(v);
+    }
+    return 4;
+}
+
+// ------------------------------------------------------------------ programs
+
+static double2 to_d2(cd z) { return make_double2(z.real(), z.imag()); }
+
+void Program::build(std::vector<DevOp> ops_in, cudaStream_t stream) {
+    ops = std::move(ops_in);
+    std::vector<double2> mats;
+    std::vector<uint32_t> u32;
+    mat_off.assign(ops.size(), 0);
+    cyc_off.assign(ops.size(), 0);
+    len_off.assign(ops.size(), 0);
+    source_gates = 0;
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const DevOp& op = ops[i];
+        source_gates += op.src_gates;
+        if (op.kind == OpKind::DENSE || op.kind == OpKind::DIAG) {
+            mat_off[i] = mats.size();
+            for (const cd& z : op.mat) mats.push_back(to_d2(z));
+        } else if (op.kind == OpKind::PERM) {
+            cyc_off[i] = u32.size();
+            u32.insert(u32.end(), op.cycles.begin(), op.cycles.end());
+            len_off[i] = u32.size();
+            u32.insert(u32.end(), op.cycle_len.begin(), op.cycle_len.end());
+        }
+    }
+    if (!mats.empty()) {
+        d_mats.ensure(mats.size() * sizeof(double2));
+        cuda_check(cudaMemcpyAsync(d_mats.ptr, mats.data(), mats.size() * sizeof(double2),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload matrices");
+    }
+    if (!u32.empty()) {
+        d_u32.ensure(u32.size() * sizeof(uint32_t));
+        cuda_check(cudaMemcpyAsync(d_u32.ptr, u32.data(), u32.size() * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload permutation cycles");
+    }
+    // the host vectors die with this scope: make sure the copies have consumed them
+    cuda_check(cudaStreamSynchronize(stream), "program upload");
+}
+
+void Program::launch_op(size_t i, const LaunchCtx& ctx, double2* st, uint32_t n,
+                        uint32_t batch) const {
+    const DevOp& op = ops[i];
+    switch (op.kind) {
+        case OpKind::K1Q: {
+            Apply1QOp a{};
+            for (int e = 0; e < 4; ++e) a.m[e] = to_d2(op.m1[e]);
+            a.t = op.targets[0];
+            a.cmask = op.cmask;
+            a.diag = op.diag1 ? 1 : 0;
+            launch_apply_1q(ctx, st, n, batch, a);
+            break;
+        }
+        case OpKind::PHASE:
+            launch_phase(ctx, st, n, batch, op.phase_mask, to_d2(op.phase));
+            break;
+        case OpKind::DENSE:
+            launch_dense(ctx, st, n, batch, op.targets.data(), op.k, op.cmask,
+                         d_mats.as<double2>() + mat_off[i]);
+            break;
+        case OpKind::DIAG:
+            launch_diag(ctx, st, n, batch, op.targets.data(), op.k, op.cmask,
+                        d_mats.as<double2>() + mat_off[i]);
+            break;
+        case OpKind::PERM: {
+            uint32_t total = 0;
+            for (uint32_t l : op.cycle_len) total += l;
+            launch_perm(ctx, st, n, batch, op.targets.data(), op.k, op.cmask,
+                        d_u32.as<uint32_t>() + cyc_off[i], d_u32.as<uint32_t>() + len_off[i],
+                        static_cast<uint32_t>(op.cycle_len.size()), total);
+            break;
+        }
+        case OpKind::PAULI:
+            launch_pauli_rotation(ctx, st, n, batch, op.x, op.zy, op.n_y, op.cos_h, op.sin_h);
+            break;
+    }
+}
+
+void Program::launch(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch) const {
+    for (size_t i = 0; i < ops.size(); ++i) launch_op(i, ctx, st, n, batch);
+}
+
+std::vector<FusedBlock> plan(const std::vector<GateDesc>& gates, uint32_t n,
+                             const FusionConfig& fc) {
+    const uint32_t w = fc.max_width ? fc.max_width : default_fusion_width();
+    if (w < 1 || w > kMaxDense) invalid("fusion width must be in [1, 6]");
+    // Barriers split the circuit into independently fused segments.
+    std::vector<FusedBlock> out;
+    std::vector<GateDesc> seg;
+    std::vector<uint32_t> seg_idx;
+    auto flush = [&]() {
+        std::vector<FusedBlock> p = plan_greedy(seg, n, w);
+        for (FusedBlock& b : p) {
+            for (uint32_t& g : b.gates) g = seg_idx[g];
+            out.push_back(std::move(b));
+        }
+        seg.clear();
+        seg_idx.clear();
+    };
+    for (uint32_t i = 0; i < gates.size(); ++i) {
+        if (gates[i].type == LQCS_GATE_BARRIER) {
+            flush();
+            continue;
+        }
+        if (!gates[i].is_unitary()) continue;
+        seg.push_back(gates[i]);
+        seg_idx.push_back(i);
+    }
+    flush();
+    return out;
+}
+
+Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
+                cudaStream_t stream) {
+    std::vector<DevOp> ops;
+    if (fc.fuse && fc.mode != 3) {
+        ops = lower_plan(plan(gates, n, fc), gates, n);
+    } else {
+        for (const GateDesc& g : gates)
+            if (g.is_unitary()) ops.push_back(lower_gate(g, n));
+    }
+    Program p;
+    p.build(std::move(ops), stream);
+    return p;
+}
+
+}  // namespace lqcs_b200
+
+// ------------------------------------------------------------------ state handle
+
+double* lqcs_state::partials(size_t values) {
+    const size_t need = (lqcs_b200::kMaxReduceBlocks + 1) * values * 2 * sizeof(double) + 4096;
+    scratch.ensure(need);
+    return scratch.as<double>();
+}
+
+void lqcs_state::sync() const {
+    lqcs_b200::cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+}
+
+namespace lqcs_b200 {
+
+double rng_uniform(Rng& r) {
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    return dist(r);
+}
+
+Rng make_rng(const lqcs_sim_options* opts) {
+    if (opts && opts->has_seed) return Rng(opts->seed);
+    return Rng(std::random_device{}());
+}
+
+uint32_t max_qubits_on_device(uint32_t batch) {
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    uint32_t q = 0;
+    while (q < 40 && (uint64_t{16} << (q + 1)) * batch <= free_b) ++q;
+    return q;
+}
+
+std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t stream) {
+    if (n == 0) invalid("Statevector: num_qubits must be >= 1");
+    if (batch == 0) invalid("state batch must be >= 1");
+    const uint32_t cap = max_qubits_on_device(batch);
+    if (n > cap || n > 40) {
+        const double gib = 16.0 * std::ldexp(1.0, static_cast<int>(n) - 30) * batch;
+        invalid("Statevector: " + std::to_string(n) + " qubits would need " +
+                std::to_string(gib) + " GiB (max " + std::to_string(cap) +
+                " qubits on this device)");
+    }
+    auto st = std::make_unique<lqcs_state>();
+    cuda_check(cudaGetDevice(&st->device), "cudaGetDevice");
+    st->n = n;
+    st->batch = batch;
+    st->stream = stream;
+    st->ctx = make_ctx(stream);
+    st->amps.ensure(sizeof(double2) * st->len() * batch);
+    launch_set_basis(st->ctx, st->d(), n, batch, 0);
+    return st;
+}
+
+void apply_circuit(lqcs_state& st, const std::vector<GateDesc>& gates, const FusionConfig& fc) {
+    std::vector<GateDesc> keep;
+    keep.reserve(gates.size());
+    for (const GateDesc& g : gates) {
+        if (g.type == LQCS_GATE_RESET)
+            invalid("run_statevector: Reset is non-deterministic; use run() instead");
+        if (g.type == LQCS_GATE_KRAUS)
+            invalid("run_statevector: noisy simulation is stochastic (one trajectory is "
+                    "not the quantum state); use run() or DensityMatrixSimulator");
+        if (g.type == LQCS_GATE_MEASURE) continue;
+        keep.push_back(g);
+    }
+    Program p = compile(keep, st.n, fc, st.stream);
+    p.launch(st.ctx, st.d(), st.n, st.batch);
+    st.sync();
+}
+
+std::unique_ptr<lqcs_program> program_create(uint32_t n, const std::vector<GateDesc>& gates,
+                                             const FusionConfig& fc) {
+    std::vector<GateDesc> keep;
+    for (const GateDesc& g : gates) {
+        if (g.type == LQCS_GATE_RESET)
+            invalid("run_statevector: Reset is non-deterministic; use run() instead");
+        if (g.type == LQCS_GATE_KRAUS)
+            invalid("run_statevector: noisy simulation is stochastic (one trajectory is "
+                    "not the quantum state); use run() or DensityMatrixSimulator");
+        if (g.type == LQCS_GATE_MEASURE) continue;
+        keep.push_back(g);
+    }
+    auto p = std::make_unique<lqcs_program>();
+    p->n = n;
+    p->prog = compile(keep, n, fc, nullptr);
+    return p;
+}
+
+void program_profile(lqcs_state& st, const lqcs_program& p, uint64_t cap, lqcs_op_profile* out,
+                     uint64_t* n_out) {
+    const size_t nops = p.prog.ops.size();
+    std::vector<cudaEvent_t> ev(nops + 1);
+    for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    cuda_check(cudaEventRecord(ev[0], st.stream), "cudaEventRecord");
+    for (size_t i = 0; i < nops; ++i) {
+        p.prog.launch_op(i, st.ctx, st.d(), st.n, st.batch);
+        cuda_check(cudaEventRecord(ev[i + 1], st.stream), "cudaEventRecord");
+    }
+    st.sync();
+    for (size_t i = 0; i < nops && i < cap && out; ++i) {
+        const DevOp& op = p.prog.ops[i];
+        float ms = 0.0f;
+        cuda_check(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "cudaEventElapsedTime");
+        lqcs_op_profile& r = out[i];
+        r.kind = static_cast<uint32_t>(op.kind);
+        r.n_targets = op.k;
+        r.n_gates = op.src_gates;
+        r.min_target = op.targets.empty() ? 0 : *std::min_element(op.targets.begin(), op.targets.end());
+        r.max_target = op.targets.empty() ? 0 : *std::max_element(op.targets.begin(), op.targets.end());
+        r.n_controls = static_cast<uint32_t>(__builtin_popcountll(op.cmask));
+        r.device_ms = ms;
+        r.alg_bytes = 32.0 * static_cast<double>(st.len()) * op.alg_fraction * st.batch;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    *n_out = nops;
+}
+
+// ------------------------------------------------------------------ reductions
+
+static double fetch1(lqcs_state& st, const double* d) {
+    double h = 0.0;
+    cuda_check(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, st.stream), "D2H");
+    st.sync();
+    return h;
+}
+
+double state_norm2(lqcs_state& st) {
+    double* part = st.partials(1);
+    double* out = part + (kMaxReduceBlocks + 1);
+    launch_norm2(st.ctx, st.d(), st.n, part, out);
+    return fetch1(st, out);
+}
+
+std::vector<double> expectation_terms(lqcs_state& st, const std::vector<PauliMasks>& terms) {
+    std::vector<double> vals(terms.size(), 0.0);
+    if (terms.empty()) return vals;
+    // group terms by x mask (one read of a_i, a_{i^x} per group of up to 8 terms)
+    std::map<uint64_t, std::vector<size_t>> groups;
+    for (size_t t = 0; t < terms.size(); ++t) groups[terms[t].x].push_back(t);
+    double* part = st.partials(2 * kMaxTermsPerPass + 1);
+    const size_t part_len = (kMaxReduceBlocks + 1) * 2 * kMaxTermsPerPass * 2;
+    DeviceBuffer d_out;
+    d_out.ensure(sizeof(double) * terms.size());
+    double* out = d_out.as<double>();
+    std::vector<size_t> order;
+    for (auto& [x, idx] : groups) {
+        for (size_t s = 0; s < idx.size(); s += kMaxTermsPerPass) {
+            const uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(kMaxTermsPerPass, idx.size() - s));
+            uint64_t zy[kMaxTermsPerPass];
+            uint32_t ny[kMaxTermsPerPass];
+            for (uint32_t c = 0; c < cnt; ++c) {
+                zy[c] = terms[idx[s + c]].zy;
+                ny[c] = terms[idx[s + c]].n_y;
+                order.push_back(idx[s + c]);
+            }
+            launch_expect_xgroup(st.ctx, st.d(), st.n, x, zy, ny, cnt, part,
+                                 out + (order.size() - cnt));
+            (void)part_len;
+        }
+    }
+    std::vector<double> packed(terms.size());
+    cuda_check(cudaMemcpyAsync(packed.data(), out, sizeof(double) * terms.size(),
+                               cudaMemcpyDeviceToHost, st.stream),
+               "D2H expectations");
+    st.sync();
+    for (size_t k = 0; k < order.size(); ++k) vals[order[k]] = packed[k];
+    return vals;
+}
+
+int collapse(lqcs_state& st, uint32_t q, double u) {
+    if (q >= st.n) out_of_range("collapse: qubit index out of range");
+    double* part = st.partials(1);
+    double* out = part + (kMaxReduceBlocks + 1);
+    launch_bitprob(st.ctx, st.d(), st.n, q, part, out);
+    const double p1 = fetch1(st, out);
+    const int outcome = u < p1 ? 1 : 0;
+    const double keep = outcome ? p1 : 1.0 - p1;
+    const double scale = 1.0 / std::sqrt(keep);
+    launch_project(st.ctx, st.d(), st.n, q, outcome, scale);
+    return outcome;
+}
+
+void reset_qubit(lqcs_state& st, uint32_t q, double u) {
+    if (!collapse(st, q, u)) return;
+    launch_move_to_zero(st.ctx, st.d(), st.n, q);
+}
+
+double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k) {
+    if (q >= st.n) out_of_range("kraus_probability: qubit index out of range");
+    double* part = st.partials(1);
+    double* out = part + (kMaxReduceBlocks + 1);
+    const double2 kk[4] = {to_d2(k[0]), to_d2(k[1]), to_d2(k[2]), to_d2(k[3])};
+    launch_kraus_prob(st.ctx, st.d(), st.n, q, kk, part, out);
+    return fetch1(st, out);
+}
+
+void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin) {
+    const uint64_t len = st.len();
+    DeviceBuffer cum, seg, du, didx, dmargin;
+    cum.ensure(sizeof(double) * len);
+    seg.ensure(sizeof(double) * (scan_block_count(st.n) + 1));
+    launch_prob_scan(st.ctx, st.d(), st.n, cum.as<double>(), seg.as<double>());
+    if (shots == 0) {
+        if (min_margin) *min_margin = 1.0;
+        st.sync();
+        return;
+    }
+    du.ensure(sizeof(double) * shots);
+    didx.ensure(sizeof(uint64_t) * shots);
+    dmargin.ensure(sizeof(double) * shots);
+    cuda_check(cudaMemcpyAsync(du.ptr, u, sizeof(double) * shots, cudaMemcpyHostToDevice,
+                               st.stream),
+               "H2D uniforms");
+    launch_sample_search(st.ctx, cum.as<double>(), st.n, du.as<double>(), shots,
+                         didx.as<uint64_t>(), dmargin.as<double>());
+    cuda_check(cudaMemcpyAsync(idx, didx.ptr, sizeof(uint64_t) * shots, cudaMemcpyDeviceToHost,
+                               st.stream),
+               "D2H sample indices");
+    std::vector<double> margins;
+    if (min_margin) {
+        margins.resize(shots);
+        cuda_check(cudaMemcpyAsync(margins.data(), dmargin.ptr, sizeof(double) * shots,
+                                   cudaMemcpyDeviceToHost, st.stream),
+                   "D2H margins");
+    }
+    st.sync();
+    if (min_margin) *min_margin = *std::min_element(margins.begin(), margins.end());
+}
+
+// ------------------------------------------------------------------ run()
+
+namespace {
+
+using Kraus = std::array<cd, 4>;
+using Channel = std::vector<Kraus>;
+
+std::vector<Channel> decode_channels(const lqcs_sim_options* opts) {
+    std::vector<Channel> out;
+    if (!opts || opts->n_channels == 0) return out;
+    if (!opts->channels) invalid("NoiseModel: channels pointer is null");
+    for (uint64_t c = 0; c < opts->n_channels; ++c) {
+        const lqcs_kraus_channel& ch = opts->channels[c];
+        if (ch.n_ops == 0 || ch.ops == nullptr) invalid("KrausChannel: needs at least one operator");
+        Channel k(ch.n_ops);
+        for (uint64_t o = 0; o < ch.n_ops; ++o)
+            for (int e = 0; e < 4; ++e) k[o][e] = cd{ch.ops[8 * o + 2 * e], ch.ops[8 * o + 2 * e + 1]};
+        out.push_back(std::move(k));
+    }
+    return out;
+}
+
+// Apply an arbitrary 2x2 to qubit q of state 0.
+void apply_matrix_1q(lqcs_state& st, uint32_t q, const Kraus& m, DeviceBuffer& tmp) {
+    if (st.n >= 5) {
+        Apply1QOp a{};
+        for (int e = 0; e < 4; ++e) a.m[e] = to_d2(m[e]);
+        a.t = q;
+        a.cmask = 0;
+        a.diag = (m[1] == cd{0, 0} && m[2] == cd{0, 0}) ? 1 : 0;
+        launch_apply_1q(st.ctx, st.d(), st.n, 1, a);
+        return;
+    }
+    tmp.ensure(4 * sizeof(double2));
+    const double2 h[4] = {to_d2(m[0]), to_d2(m[1]), to_d2(m[2]), to_d2(m[3])};
+    cuda_check(cudaMemcpyAsync(tmp.ptr, h, sizeof(h), cudaMemcpyHostToDevice, st.stream), "H2D");
+    launch_dense(st.ctx, st.d(), st.n, 1, &q, 1, 0, tmp.as<double2>());
+    st.sync();
+}
+
+// sample_kraus_branch (src/backend/statevector_simulator.cpp:122-144): one uniform, branch
+// probabilities ||K_i psi||^2 (here all from one reduced density matrix of qubit q),
+// skip p <= 0, choose the first i with u < cumulative p, fall back to the last non-zero
+// branch, apply K_i / sqrt(p_i).
+void sample_kraus_branch(lqcs_state& st, const Channel& ch, uint32_t q, double u,
+                         DeviceBuffer& tmp) {
+    double* part = st.partials(4);
+    double* out = part + (kMaxReduceBlocks + 1) * 4;
+    launch_rdm1(st.ctx, st.d(), st.n, q, part, out);
+    double r[4];
+    cuda_check(cudaMemcpyAsync(r, out, sizeof(r), cudaMemcpyDeviceToHost, st.stream), "D2H rdm");
+    st.sync();
+    const cd rho00{r[0], 0.0}, rho11{r[1], 0.0}, rho01{r[2], r[3]}, rho10 = std::conj(rho01);
+    double cum = 0.0;
+    int chosen = -1;
+    double chosen_p = 0.0;
+    for (size_t i = 0; i < ch.size(); ++i) {
+        const Kraus& k = ch[i];
+        // Tr(K rho K^dagger) = sum_r sum_{c,c'} K[r][c] rho[c][c'] conj(K[r][c'])
+        cd p{0.0, 0.0};
+        for (int row = 0; row < 2; ++row) {
+            const cd k0 = k[2 * row], k1 = k[2 * row + 1];
+            p += k0 * rho00 * std::conj(k0) + k0 * rho01 * std::conj(k1) +
+                 k1 * rho10 * std::conj(k0) + k1 * rho11 * std::conj(k1);
+        }
+        const double pr = p.real();
+        if (pr <= 0.0) continue;
+        chosen = static_cast<int>(i);
+        chosen_p = pr;
+        cum += pr;
+        if (u < cum) break;
+    }
+    if (chosen < 0) return;
+    const double inv = 1.0 / std::sqrt(chosen_p);
+    const Kraus& k = ch[chosen];
+    const Kraus m{k[0] * inv, k[1] * inv, k[2] * inv, k[3] * inv};
+    apply_matrix_1q(st, q, m, tmp);
+}
+
+// Emission order of SingleQubitGateFusion (src/transpiler/gate_fusion.cpp:32-67), reduced
+// to what run()'s path selection reads from it: true when some unitary is emitted after a
+// Measure.  Pending one-qubit products are flushed on any other instruction touching the
+// qubit, on Barrier, and at the end; identity products (within 1e-12) are dropped.
+bool fused_has_unitary_after_measure(const std::vector<GateDesc>& gates, uint32_t n) {
+    using M2 = std::array<cd, 4>;
+    std::vector<std::optional<M2>> pending(n);
+    bool seen_measure = false, after = false;
+    auto is_identity = [](const M2& m) {
+        constexpr double tol = 1e-12;
+        return std::abs(m[0] - cd{1, 0}) < tol && std::abs(m[1]) < tol && std::abs(m[2]) < tol &&
+               std::abs(m[3] - cd{1, 0}) < tol;
+    };
+    auto emit_unitary = [&]() { if (seen_measure) after = true; };
+    auto flush = [&](uint32_t q) {
+        if (!pending[q]) return;
+        if (!is_identity(*pending[q])) emit_unitary();
+        pending[q].reset();
+    };
+    for (const GateDesc& g : gates) {
+        if (g.is_unitary() && g.n_controls == 0 && g.base_qubits() == 1) {
+            const std::vector<cd> m = g.base_matrix();
+            const M2 a{m[0], m[1], m[2], m[3]};
+            const uint32_t q = g.qubits[0];
+            if (pending[q]) {
+                const M2& b = *pending[q];
+                pending[q] = M2{a[0] * b[0] + a[1] * b[2], a[0] * b[1] + a[1] * b[3],
+                                a[2] * b[0] + a[3] * b[2], a[2] * b[1] + a[3] * b[3]};
+            } else {
+                pending[q] = a;
+            }
+            continue;
+        }
+        if (g.type == LQCS_GATE_BARRIER) {
+            for (uint32_t q = 0; q < n; ++q) flush(q);
+        } else {
+            for (uint32_t q : g.qubits) flush(q);
+        }
+        if (g.type == LQCS_GATE_MEASURE) seen_measure = true;
+        else if (g.is_unitary()) emit_unitary();
+    }
+    for (uint32_t q = 0; q < n; ++q) flush(q);
+    return after;
+}
+
+}  // namespace
+
+void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,
+               uint64_t shots, const lqcs_sim_options* opts, uint64_t* regs) {
+    if (shots == 0) invalid("run: shots must be >= 1");
+    if (n_clbits > 64) invalid("run: this engine reports at most 64 classical bits");
+    const std::vector<Channel> channels = decode_channels(opts);
+    const bool noisy = !channels.empty();
+    const bool fuse = opts ? (opts->fuse_gates != 0) : true;
+
+    // Path selection of StatevectorSimulator::run (src/backend/statevector_simulator.cpp:241-257),
+    // evaluated on the instruction order the reference's fusion pass would emit.
+    bool seen_measure = false, per_shot = noisy;
+    for (const GateDesc& g : gates) {
+        if (g.type == LQCS_GATE_MEASURE) {
+            if (g.clbit >= n_clbits) {
+                out_of_range("clbit index " + std::to_string(g.clbit) +
+                             " out of range (num_clbits = " + std::to_string(n_clbits) + ")");
+            }
+            seen_measure = true;
+        } else if (g.type == LQCS_GATE_RESET || g.type == LQCS_GATE_KRAUS) {
+            per_shot = true;
+        } else if (seen_measure && g.is_unitary()) {
+            per_shot = true;
+        }
+    }
+    if (!per_shot && fuse && !noisy) per_shot = fused_has_unitary_after_measure(gates, n);
+    if (!seen_measure) {
+        invalid("run: circuit has no measurements; use run_statevector() to inspect the final "
+                "state");
+    }
+    Rng rng = make_rng(opts);
+    FusionConfig fc;
+    fc.fuse = fuse && !noisy;
+    if (opts) {
+        fc.max_width = static_cast<uint32_t>(std::max(0, opts->max_fusion_width));
+        fc.mode = opts->fusion_mode;
+    }
+    auto st = new_state(n, 1, nullptr);
+
+    if (!per_shot) {
+        // run_sampling (src/backend/statevector_simulator.cpp:88-119)
+        apply_circuit(*st, gates, fc);
+        std::vector<int64_t> src(n_clbits, -1);
+        for (const GateDesc& g : gates)
+            if (g.type == LQCS_GATE_MEASURE) src[g.clbit] = g.qubits[0];
+        std::vector<double> u(shots);
+        for (uint64_t s = 0; s < shots; ++s) u[s] = rng_uniform(rng);
+        std::vector<uint64_t> idx(shots);
+        sample(*st, u.data(), shots, idx.data(), nullptr);
+        for (uint64_t s = 0; s < shots; ++s) {
+            uint64_t reg = 0;
+            for (uint32_t c = 0; c < n_clbits; ++c)
+                if (src[c] >= 0 && ((idx[s] >> src[c]) & 1u)) reg |= uint64_t{1} << c;
+            regs[s] = reg;
+        }
+        return;
+    }
+
+    // run_per_shot (src/backend/statevector_simulator.cpp:156-190): compile the unitary
+    // stretches between non-unitary instructions once; noisy circuits keep one gate per
+    // stretch because noise follows every gate.
+    struct Item {
+        int kind;          // 0 unitary program, 1 measure, 2 reset, 3 kraus
+        size_t prog = 0;
+        uint32_t q = 0, clbit = 0;
+        std::vector<uint32_t> noise_qubits;
+        Channel kraus;
+    };
+    std::vector<Program> progs;
+    std::vector<Item> items;
+    std::vector<GateDesc> stretch;
+    auto flush_stretch = [&]() {
+        if (stretch.empty()) return;
+        progs.push_back(compile(stretch, n, fc, st->stream));
+        Item it;
+        it.kind = 0;
+        it.prog = progs.size() - 1;
+        items.push_back(std::move(it));
+        stretch.clear();
+    };
+    for (const GateDesc& g : gates) {
+        if (g.type == LQCS_GATE_BARRIER) continue;
+        if (g.type == LQCS_GATE_MEASURE || g.type == LQCS_GATE_RESET || g.type == LQCS_GATE_KRAUS) {
+            flush_stretch();
+            Item it;
+            it.kind = g.type == LQCS_GATE_MEASURE ? 1 : g.type == LQCS_GATE_RESET ? 2 : 3;
+            it.q = g.qubits[0];
+            it.clbit = g.clbit;
+            if (it.kind == 3) it.kraus.assign(g.kraus.begin(), g.kraus.end());
+            items.push_back(std::move(it));
+            continue;
+        }
+        stretch.push_back(g);
+        if (noisy) {
+            flush_stretch();
+            items.back().noise_qubits = g.qubits;
+        }
+    }
+    flush_stretch();
+
+    DeviceBuffer tmp;
+    for (uint64_t s = 0; s < shots; ++s) {
+        launch_set_basis(st->ctx, st->d(), n, 1, 0);
+        uint64_t creg = 0;
+        for (const Item& it : items) {
+            switch (it.kind) {
+                case 0:
+                    progs[it.prog].launch(st->ctx, st->d(), n, 1);
+                    for (const Channel& ch : channels)
+                        for (uint32_t q : it.noise_qubits)
+                            sample_kraus_branch(*st, ch, q, rng_uniform(rng), tmp);
+                    break;
+                case 1: {
+                    const int out = collapse(*st, it.q, rng_uniform(rng));
+                    if (out) creg |= uint64_t{1} << it.clbit;
+                    else creg &= ~(uint64_t{1} << it.clbit);
+                    break;
+                }
+                case 2:
+                    reset_qubit(*st, it.q, rng_uniform(rng));
+                    break;
+                case 3:
+                    sample_kraus_branch(*st, it.kraus, it.q, rng_uniform(rng), tmp);
+                    break;
+            }
+        }
+        regs[s] = creg;
+    }
+    st->sync();
+}
+
+// ------------------------------------------------------------------ Hamiltonians
+
+Hamiltonian decode_hamiltonian(const lqcs_hamiltonian* h, uint32_t n) {
+    if (!h) invalid("hamiltonian is null");
+    Hamiltonian out;
+    if (h->n_terms > 0 && (!h->coeffs || !h->paulis)) invalid("hamiltonian: null arrays");
+    for (uint64_t t = 0; t < h->n_terms; ++t) {
+        out.coeffs.push_back(h->coeffs[t]);
+        out.terms.push_back(pauli_global_masks(h->paulis[t], n, "expectation_value"));
+    }
+    return out;
+}
+
+double energy(lqcs_state& st, const Hamiltonian& h) {
+    // algorithms::expectation (src/algorithms/vqe.cpp:11-17): sum in term order
+    const std::vector<double> v = expectation_terms(st, h.terms);
+    double e = 0.0;
+    for (size_t t = 0; t < v.size(); ++t) e += h.coeffs[t] * v[t];
+    return e;
+}
+
+std::vector<GateDesc> bind_params(const std::vector<GateDesc>& tmpl,
+                                         const std::vector<uint64_t>& param_inst,
+                                         const double* values) {
+    std::vector<GateDesc> g = tmpl;
+    for (size_t p = 0; p < param_inst.size(); ++p) {
+        GateDesc& d = g[param_inst[p]];
+        if (d.params.empty()) d.params.push_back(0.0);
+        d.params[0] = values[p];
+    }
+    return g;
+}
+
+void check_pc(const lqcs_parametric_circuit* pc, std::vector<GateDesc>& tmpl,
+                     std::vector<uint64_t>& pinst) {
+    if (!pc) invalid("parametric circuit is null");
+    tmpl = decode_all(pc->insts, pc->n_insts, pc->n_qubits);
+    if (pc->n_params > 0 && !pc->param_inst) invalid("parametric circuit: null param_inst");
+    pinst.assign(pc->param_inst, pc->param_inst + pc->n_params);
+    for (uint64_t p : pinst) {
+        if (p >= tmpl.size()) invalid("parametric circuit: parameter index out of range");
+        const GateDesc& g = tmpl[p];
+        const bool ok = (g.type == LQCS_GATE_RX || g.type == LQCS_GATE_RY || g.type == LQCS_GATE_RZ ||
+                         g.type == LQCS_GATE_PAULI_ROTATION) && g.n_controls == 0;
+        if (!ok) invalid("parametric circuit: parameterised gates must be RX, RY, RZ or rp");
+    }
+}
+
+void parameter_shift(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
+                     const double* params, double* grad) {
+    // algorithms::parameter_shift_gradient (src/algorithms/vqe.cpp:68-94)
+    std::vector<GateDesc> tmpl;
+    std::vector<uint64_t> pinst;
+    check_pc(pc, tmpl, pinst);
+    const size_t np = pinst.size();
+    auto st = new_state(pc->n_qubits, 1, nullptr);
+    FusionConfig fc;
+    std::vector<double> theta(params, params + np);
+    auto e_at = [&](const std::vector<double>& th) {
+        launch_set_basis(st->ctx, st->d(), st->n, 1, 0);
+        apply_circuit(*st, bind_params(tmpl, pinst, th.data()), fc);
+        return energy(*st, h);
+    };
+    constexpr double half_pi = std::numbers::pi / 2;
+    for (size_t k = 0; k < np; ++k) {
+        const double saved = theta[k];
+        theta[k] = saved + half_pi;
+        const double ep = e_at(theta);
+        theta[k] = saved - half_pi;
+        const double em = e_at(theta);
+        theta[k] = saved;
+        grad[k] = 0.5 * (ep - em);
+    }
+}
+
+}  // namespace lqcs_b200

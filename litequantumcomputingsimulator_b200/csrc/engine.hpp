@@ -1,0 +1,147 @@
+// engine.hpp — device runtime of the engine: state handles, compiled op programs, and
+// the run paths of StatevectorSimulator (end-of-circuit sampling, per-shot evolution,
+// trajectory noise) plus expectations and gradients.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "gates.hpp"
+#include "kernels.cuh"
+
+namespace lqcs_b200 {
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Owning device allocation.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            bytes = o.bytes;
+            o.ptr = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DeviceBuffer() { release(); }
+    void release();
+    void ensure(size_t b);
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+int device_sm_count();
+LaunchCtx make_ctx(cudaStream_t s);
+
+// A compiled sequence of device ops with its constant data resident on the device.
+struct Program {
+    std::vector<DevOp> ops;
+    std::vector<uint64_t> mat_off;   // per op: offset (double2) of its matrix / diagonal
+    std::vector<uint64_t> cyc_off;   // per op: offset (uint32) of its cycles
+    std::vector<uint64_t> len_off;   // per op: offset (uint32) of its cycle lengths
+    DeviceBuffer d_mats, d_u32;
+    uint64_t source_gates = 0;
+
+    void build(std::vector<DevOp> ops_in, cudaStream_t stream);
+    void launch(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch) const;
+    void launch_op(size_t i, const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch) const;
+};
+
+// Fusion knobs.
+struct FusionConfig {
+    bool fuse = true;
+    uint32_t max_width = 0;   // 0 = engine default
+    int mode = 0;             // 0 default, 1 greedy, 2 learned, 3 none
+};
+uint32_t default_fusion_width();
+
+// Compile a list of unitary gates to a Program (fused or gate by gate).
+Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
+                cudaStream_t stream);
+std::vector<FusedBlock> plan(const std::vector<GateDesc>& gates, uint32_t n,
+                             const FusionConfig& fc);
+
+}  // namespace lqcs_b200
+
+// The opaque handle of the C ABI.
+struct lqcs_state {
+    int device = 0;
+    uint32_t n = 0;
+    uint32_t batch = 1;
+    cudaStream_t stream = nullptr;
+    lqcs_b200::DeviceBuffer amps;
+    lqcs_b200::DeviceBuffer scratch;   // reductions (device)
+    lqcs_b200::LaunchCtx ctx;
+
+    double2* d() const { return amps.as<double2>(); }
+    uint64_t len() const { return uint64_t{1} << n; }
+    double* partials(size_t values);   // scratch for `values` reduced outputs
+    void sync() const;
+};
+
+// A compiled circuit handle of the C ABI.
+struct lqcs_program {
+    uint32_t n = 0;
+    lqcs_b200::Program prog;
+};
+
+namespace lqcs_b200 {
+
+std::unique_ptr<lqcs_program> program_create(uint32_t n, const std::vector<GateDesc>& gates,
+                                             const FusionConfig& fc);
+void program_profile(lqcs_state& st, const lqcs_program& p, uint64_t cap, lqcs_op_profile* out,
+                     uint64_t* n_out);
+
+using Rng = std::mt19937_64;
+// One draw of lqcs::Rng::uniform (include/lqcs/core/random.hpp:10-23):
+// std::uniform_real_distribution<double>(0, 1) over std::mt19937_64.
+double rng_uniform(Rng& r);
+Rng make_rng(const lqcs_sim_options* opts);
+
+std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t stream);
+uint32_t max_qubits_on_device(uint32_t batch);
+
+// Apply unitary instructions (skip Measure/Barrier, reject Reset).
+void apply_circuit(lqcs_state& st, const std::vector<GateDesc>& gates, const FusionConfig& fc);
+
+// Reductions on state 0 of a handle.
+double state_norm2(lqcs_state& st);
+std::vector<double> expectation_terms(lqcs_state& st, const std::vector<PauliMasks>& terms);
+int collapse(lqcs_state& st, uint32_t q, double u);
+void reset_qubit(lqcs_state& st, uint32_t q, double u);
+double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k);
+void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin);
+
+// StatevectorSimulator::run.
+void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,
+               uint64_t shots, const lqcs_sim_options* opts, uint64_t* regs);
+
+// Gradients.
+struct Hamiltonian {
+    std::vector<double> coeffs;
+    std::vector<PauliMasks> terms;
+};
+Hamiltonian decode_hamiltonian(const lqcs_hamiltonian* h, uint32_t n);
+double energy(lqcs_state& st, const Hamiltonian& h);
+// Decode a parametric circuit; parameterised gates must be RX, RY, RZ or rp without controls.
+void check_pc(const lqcs_parametric_circuit* pc, std::vector<GateDesc>& tmpl,
+              std::vector<uint64_t>& pinst);
+// ParametricCircuit::bind (src/circuit/parametric_circuit.cpp:73-96).
+std::vector<GateDesc> bind_params(const std::vector<GateDesc>& tmpl,
+                                  const std::vector<uint64_t>& param_inst, const double* values);
+void parameter_shift(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
+                     const double* params, double* grad);
+void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
+                     const double* params, uint64_t batch, uint32_t max_resident,
+                     double* energy_out, double* grad_out);
+
+}  // namespace lqcs_b200

@@ -1,0 +1,318 @@
+"""GPU parity: the engine's CUDA path against the oracle (the C restatement and the
+reference library itself) on the same seeded inputs.
+
+Tolerances: amplitudes within 1e-12 (absolute, per amplitude) of the CPU path; counts
+identical given the same seed; expectation values within 1e-12; gradients within 1e-9 of
+the reference's parameter-shift gradient.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import litequantumcomputingsimulator_b200 as lq
+from litequantumcomputingsimulator_b200 import workloads as W
+
+from helpers import random_circuit, random_unitary
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def engine_state(qc, fuse=False, width=0, init=None):
+    if init is None:
+        sim = lq.StatevectorSimulator(fuse_gates=fuse, max_fusion_width=width)
+        return sim.run_statevector(qc).to_numpy()
+    sv = lq.Statevector.from_numpy(init)
+    sv.apply(qc, fuse_gates=fuse, max_fusion_width=width)
+    return sv.to_numpy()
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 9])
+@pytest.mark.parametrize("seed", [1, 2])
+def test_every_gate_type_unfused(port, n, seed):
+    qc = random_circuit(n, 60, seed=100 * n + seed)
+    want = port.run_statevector(qc, fuse=False)
+    got = engine_state(qc, fuse=False)
+    assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("n", [3, 6, 8, 11])
+@pytest.mark.parametrize("width", [1, 2, 3, 4, 5, 6])
+def test_fused_blocks_match(port, n, width):
+    qc = random_circuit(n, 80, seed=7 * n + width)
+    want = port.run_statevector(qc, fuse=False)
+    got = engine_state(qc, fuse=True, width=min(width, n))
+    assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("n", [5, 7, 12])
+def test_from_random_state(port, n):
+    init = W.gaussian_state(n, seed=3)
+    qc = random_circuit(n, 40, seed=n)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    for fuse in (False, True):
+        got = engine_state(qc, fuse=fuse, init=init)
+        assert np.max(np.abs(got - want)) < TOL
+
+
+def test_single_qubit_every_target_and_control(port):
+    n = 11
+    init = W.gaussian_state(n, seed=11)
+    rng = np.random.default_rng(0)
+    for t in range(n):
+        qc = lq.QuantumCircuit(n)
+        qc.u(*rng.uniform(0, 2 * math.pi, 3), t)
+        qc.rz(0.3, t).t(t).p(0.7, t)
+        for c in range(n):
+            if c != t:
+                qc.cx(c, t).cp(0.4, c, t).crx(0.9, c, t)
+        want = port.run_statevector(qc, fuse=False, state=init)
+        got = engine_state(qc, fuse=False, init=init)
+        assert np.max(np.abs(got - want)) < TOL, t
+
+
+def test_two_qubit_and_block_every_pair(port):
+    n = 8
+    init = W.gaussian_state(n, seed=5)
+    rng = np.random.default_rng(1)
+    qc = lq.QuantumCircuit(n)
+    for a in range(n):
+        for b in range(n):
+            if a != b:
+                qc.unitary(random_unitary(2, rng), [a, b])
+                qc.swap(a, b)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    got = engine_state(qc, fuse=False, init=init)
+    assert np.max(np.abs(got - want)) < TOL
+
+
+def test_matches_reference_library(ref):
+    for n, seed in [(4, 1), (9, 2), (13, 3)]:
+        qc = random_circuit(n, 50, seed=seed)
+        want = ref.run_statevector(qc, fuse=True)
+        for fuse in (False, True):
+            got = engine_state(qc, fuse=fuse)
+            assert np.max(np.abs(got - want)) < TOL
+
+
+def test_brickwork_20q_reference(ref):
+    qc = W.brickwork(20, 20, seed=2024)
+    want = ref.run_statevector(qc, fuse=True)
+    for width in (0, 2, 4, 5):
+        got = engine_state(qc, fuse=True, width=width)
+        assert np.max(np.abs(got - want)) < TOL
+
+
+def test_qft_random_state(ref):
+    n = 14
+    init = W.gaussian_state(n, seed=9)
+    qc = lq.algorithms.qft(n)
+    want = ref.evolve_from(qc, init)
+    for fuse in (False, True):
+        got = engine_state(qc, fuse=fuse, init=init)
+        assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("n,depth,shots,seed", [(2, 1, 4096, 42), (10, 6, 4096, 123),
+                                                (16, 10, 8192, 9), (20, 20, 4096, 2024)])
+def test_sampling_counts_identical(ref, n, depth, shots, seed):
+    qc = W.brickwork(n, depth, seed=seed + 1, measure=True)
+    want = ref.run(qc, shots, seed)
+    got_regs = lq.StatevectorSimulator(seed=seed).run_registers(qc, shots)
+    vals, cnt = np.unique(got_regs, return_counts=True)
+    got = {int(v): int(c) for v, c in zip(vals, cnt)}
+    assert got == want
+
+
+def test_sample_margin_and_upper_bound(port):
+    n = 12
+    init = W.gaussian_state(n, seed=4)
+    sv = lq.Statevector.from_numpy(init)
+    u = W.UniformStream(77).take(5000)
+    idx, margin = sv.sample(u)
+    cum = np.cumsum(np.abs(init) ** 2)
+    total = cum[-1]
+    want = np.searchsorted(cum, u * total, side="right")
+    assert np.array_equal(idx.astype(np.int64), want)
+    assert margin > 0
+
+
+def test_counts_fusion_on_off_identical():
+    qc = lq.QuantumCircuit(3, 3)
+    qc.h(0).t(0).cx(0, 1).rx(0.4, 2).sx(2).cx(1, 2).measure_all()
+    on = lq.StatevectorSimulator(seed=5, fuse_gates=True).run(qc, 512).counts()
+    off = lq.StatevectorSimulator(seed=5, fuse_gates=False).run(qc, 512).counts()
+    assert on == off
+
+
+def test_measurement_format_and_mapping():
+    qc = lq.QuantumCircuit(2, 2)
+    qc.x(0).measure(0, 1)
+    r = lq.StatevectorSimulator(seed=5).run(qc, 10)
+    assert r.counts() == {"10": 10}
+    qc = lq.QuantumCircuit(1, 1)
+    qc.x(0).measure(0, 0)
+    assert lq.StatevectorSimulator(seed=7).run(qc, 100).counts() == {"1": 100}
+
+
+@pytest.mark.parametrize("seed", [42, 7, 11])
+def test_midcircuit_and_reset_counts_identical(ref, seed):
+    circuits = []
+    a = lq.QuantumCircuit(2, 2)
+    a.h(0).measure(0, 0).cx(0, 1).measure(1, 1)
+    circuits.append(a)
+    b = lq.QuantumCircuit(1, 2)
+    b.h(0).measure(0, 0).h(0).measure(0, 1)
+    circuits.append(b)
+    c = lq.QuantumCircuit(2, 2)
+    c.h(0).cx(0, 1).reset(0).measure_all()
+    circuits.append(c)
+    d = lq.QuantumCircuit(6, 6)
+    d.h(0).cx(0, 3).ry(0.3, 5).measure(3, 2).reset(3).cx(5, 3).h(1).measure_all()
+    circuits.append(d)
+    for qc in circuits:
+        want = ref.run(qc, 512, seed)
+        regs = lq.StatevectorSimulator(seed=seed).run_registers(qc, 512)
+        vals, cnt = np.unique(regs, return_counts=True)
+        assert {int(v): int(c) for v, c in zip(vals, cnt)} == want
+
+
+def test_trajectory_counts_identical(ref):
+    noise = lq.NoiseModel()
+    noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.15))
+    noise.add_all_qubit_channel(lq.KrausChannel.amplitude_damping(0.1))
+    qc = lq.QuantumCircuit(3, 3)
+    qc.h(0).cx(0, 1).t(1).cx(1, 2).measure_all()
+    want = ref.run(qc, 400, 99, noise=noise)
+    regs = lq.StatevectorSimulator(seed=99, noise=noise).run_registers(qc, 400)
+    vals, cnt = np.unique(regs, return_counts=True)
+    got = {int(v): int(c) for v, c in zip(vals, cnt)}
+    assert got == want
+
+
+def test_trajectory_matches_density_matrix(ref):
+    noise = lq.NoiseModel()
+    noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.15))
+    qc = lq.QuantumCircuit(2, 2)
+    qc.h(0).cx(0, 1).t(1).cx(1, 0).measure_all()
+    shots = 20000
+    counts = lq.StatevectorSimulator(seed=99, noise=noise).run(qc, shots).counts()
+    exact = ref.dm_probabilities(qc, noise)
+    for i, key in enumerate(["00", "01", "10", "11"]):
+        assert abs(counts.get(key, 0) / shots - exact[i]) < 0.0125
+
+
+@pytest.mark.parametrize("n", [3, 8, 14])
+def test_expectation_values(port, n):
+    init = W.gaussian_state(n, seed=n)
+    sv = lq.Statevector.from_numpy(init)
+    rng = np.random.default_rng(n)
+    paulis = ["".join("IXYZ"[i] for i in rng.integers(0, 4, n)) for _ in range(40)]
+    got = lq.algorithms.expectation_terms(sv, paulis)
+    want = np.array([port.expectation_value(init, p) for p in paulis])
+    assert np.max(np.abs(got - want)) < TOL
+    h = [(float(rng.standard_normal()), p) for p in paulis]
+    assert abs(lq.algorithms.expectation(sv, h) - port.expectation(init, h)) < 1e-11
+
+
+def test_known_expectations():
+    qc = lq.QuantumCircuit(2)
+    qc.h(0).cx(0, 1)
+    sv = lq.StatevectorSimulator().run_statevector(qc)
+    assert abs(sv.expectation_value("ZZ") - 1) < TOL
+    assert abs(sv.expectation_value("XX") - 1) < TOL
+    assert abs(sv.expectation_value("YY") + 1) < TOL
+    assert abs(sv.expectation_value("ZI")) < TOL
+
+
+@pytest.mark.parametrize("n", [3, 9])
+def test_collapse_reset_kraus(port, n):
+    from oracle.oracle import _PortLib
+    lib = _PortLib.get()
+    init = W.gaussian_state(n, seed=21)
+    for q in range(n):
+        for u in (0.1, 0.9):
+            a = init.copy()
+            o_want = lib.orc_collapse_qubit(a.ctypes.data, a.size, q, u)
+            sv = lq.Statevector.from_numpy(init)
+            o_got = sv.collapse(q, u)
+            assert o_got == o_want
+            assert np.max(np.abs(sv.to_numpy() - a)) < TOL
+            b = init.copy()
+            lib.orc_reset_qubit(b.ctypes.data, b.size, q, u)
+            sv = lq.Statevector.from_numpy(init)
+            sv.reset_qubit(q, u)
+            assert np.max(np.abs(sv.to_numpy() - b)) < TOL
+        for ch in (lq.KrausChannel.depolarizing(0.3), lq.KrausChannel.amplitude_damping(0.4)):
+            for k in ch.ops:
+                kk = np.ascontiguousarray(np.asarray(k, dtype=np.complex128))
+                want = lib.orc_kraus_probability(init.ctypes.data, init.size, q, kk.ctypes.data)
+                got = lq.Statevector.from_numpy(init).kraus_probability(q, kk)
+                assert abs(got - want) < TOL
+
+
+def test_parameter_shift_matches_reference(ref):
+    pc, theta = W.random_pauli_ansatz(6, 20, seed=5)
+    h = W.random_hamiltonian(6, 30, seed=6)
+    want = ref.parameter_shift_gradient(h, pc, theta)
+    got = np.array(lq.algorithms.parameter_shift_gradient(h, pc, theta))
+    assert np.max(np.abs(got - want)) < 1e-9
+
+
+@pytest.mark.parametrize("n", [3, 7])
+def test_adjoint_matches_parameter_shift_and_fd(ref, n):
+    pc, theta = W.random_pauli_ansatz(n, 16, seed=n, max_w=min(8, n))
+    h = W.random_hamiltonian(n, 25, seed=n + 1)
+    want = ref.parameter_shift_gradient(h, pc, theta)
+    e, g = lq.algorithms.adjoint_gradient(h, pc, theta)
+    assert np.max(np.abs(g - want)) < 1e-9
+    e_ref = ref.expectation(ref.run_statevector(pc.bind(theta)), h)
+    assert abs(e - e_ref) < 1e-11
+    hstep = 1e-4
+    for k in range(0, len(theta), 5):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += hstep
+        tm[k] -= hstep
+        ep = ref.expectation(ref.run_statevector(pc.bind(tp)), h)
+        em = ref.expectation(ref.run_statevector(pc.bind(tm)), h)
+        assert abs(g[k] - (ep - em) / (2 * hstep)) < 1e-6
+
+
+def test_adjoint_batched_equals_single(ref):
+    pc, _ = W.random_pauli_ansatz(8, 24, seed=8)
+    h = W.random_hamiltonian(8, 40, seed=9)
+    sets = W.random_parameter_sets(pc.num_parameters(), 10, seed=10)
+    e_b, g_b = lq.algorithms.adjoint_gradient(h, pc, sets, max_resident=4)
+    for b in range(sets.shape[0]):
+        e1, g1 = lq.algorithms.adjoint_gradient(h, pc, sets[b])
+        assert abs(e1 - e_b[b]) < 1e-12
+        assert np.max(np.abs(g1 - g_b[b])) < 1e-12
+    want = ref.parameter_shift_gradient(h, pc, sets[3])
+    assert np.max(np.abs(g_b[3] - want)) < 1e-9
+
+
+def test_errors_match_reference_types():
+    sim = lq.StatevectorSimulator()
+    qc = lq.QuantumCircuit(2)
+    qc.h(0)
+    with pytest.raises(ValueError, match="no measurements"):
+        sim.run(qc, 10)
+    qc.measure_all()
+    with pytest.raises(ValueError, match="shots must be >= 1"):
+        sim.run(qc, 0)
+    r = lq.QuantumCircuit(1, 1)
+    r.reset(0)
+    with pytest.raises(ValueError, match="Reset is non-deterministic"):
+        sim.run_statevector(r)
+    noise = lq.NoiseModel()
+    noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.1))
+    with pytest.raises(ValueError, match="stochastic"):
+        lq.StatevectorSimulator(noise=noise).run_statevector(lq.QuantumCircuit(1).h(0))
+    with pytest.raises(ValueError):
+        lq.Statevector(60)
+    sv = lq.Statevector(2)
+    with pytest.raises(IndexError):
+        _ = sv[4]
+    with pytest.raises(ValueError, match="length must equal"):
+        sv.expectation_value("ZZZ")
