@@ -501,6 +501,30 @@ std::vector<FusedBlock> plan_greedy(const std::vector<GateDesc>& gates, uint32_t
         alive.push_back(true);
     }
     for (int b = 0; b < static_cast<int>(open.size()); ++b) close(b);
+    return pack_consecutive(out, max_width);
+}
+
+std::vector<FusedBlock> pack_consecutive(const std::vector<FusedBlock>& blocks,
+                                         uint32_t max_width) {
+    // Two blocks adjacent in a valid emission order can always be concatenated; their
+    // gates keep program order within the merged block.
+    std::vector<FusedBlock> out;
+    for (const FusedBlock& b : blocks) {
+        if (!out.empty()) {
+            FusedBlock& last = out.back();
+            std::vector<uint32_t> uni = last.qubits;
+            uni.insert(uni.end(), b.qubits.begin(), b.qubits.end());
+            std::sort(uni.begin(), uni.end());
+            uni.erase(std::unique(uni.begin(), uni.end()), uni.end());
+            if (uni.size() <= max_width) {
+                last.qubits = std::move(uni);
+                last.gates.insert(last.gates.end(), b.gates.begin(), b.gates.end());
+                std::sort(last.gates.begin(), last.gates.end());
+                continue;
+            }
+        }
+        out.push_back(b);
+    }
     return out;
 }
 

@@ -109,6 +109,10 @@ struct FusedBlock {
 std::vector<FusedBlock> plan_greedy(const std::vector<GateDesc>& gates, uint32_t n,
                                     uint32_t max_width);
 
+// Merge neighbouring blocks of an emission order while their qubit union fits max_width.
+std::vector<FusedBlock> pack_consecutive(const std::vector<FusedBlock>& blocks,
+                                         uint32_t max_width);
+
 // Dense matrix of a block (block-local bit j <-> qubits[j]).
 std::vector<cd> block_matrix(const FusedBlock& b, const std::vector<GateDesc>& gates);
 
