@@ -133,6 +133,8 @@ SIGNATURES = {
     "lqcs_state_expectation_pauli": (C.c_int, [StatePtr, C.c_char_p, _P(C.c_double)]),
     "lqcs_state_expectation_terms": (C.c_int, [StatePtr, _P(C.c_char_p), C.c_void_p, C.c_uint64,
                                                C.c_void_p, _P(C.c_double)]),
+    "lqcs_expectation_terms_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, _P(C.c_char_p),
+                                                 C.c_uint64, C.c_void_p, C.c_void_p]),
     "lqcs_state_collapse": (C.c_int, [StatePtr, C.c_uint32, C.c_double, _P(C.c_int32)]),
     "lqcs_state_reset_qubit": (C.c_int, [StatePtr, C.c_uint32, C.c_double]),
     "lqcs_state_kraus_probability": (C.c_int, [StatePtr, C.c_uint32, C.c_void_p,

@@ -325,6 +325,15 @@ int lqcs_state_expectation_terms(const lqcs_state* st, const char* const* paulis
     });
 }
 
+int lqcs_expectation_terms_noalloc(const void* d_amps, uint32_t n_qubits,
+                                   const char* const* paulis, uint64_t n_terms,
+                                   double* host_values, void* stream) {
+    return guarded([&] {
+        lqcs_b200::expectation_terms_static(d_amps, n_qubits, paulis, n_terms, host_values,
+                                            static_cast<cudaStream_t>(stream));
+    });
+}
+
 int lqcs_state_collapse(lqcs_state* st, uint32_t qubit, double uniform, int32_t* outcome) {
     return guarded([&] {
         need(st, "state");

@@ -121,6 +121,11 @@ void reset_qubit(lqcs_state& st, uint32_t q, double u);
 double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k);
 void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin);
 
+// Expectation values with the scratch in a static device array (static_expect.cu).
+uint32_t static_expectation_max_terms();
+void expectation_terms_static(const void* d_amps, uint32_t n_qubits, const char* const* paulis,
+                              uint64_t n_terms, double* host_values, cudaStream_t stream);
+
 // StatevectorSimulator::run.
 void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,
                uint64_t shots, const lqcs_sim_options* opts, uint64_t* regs);
