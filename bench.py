@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--fusion-mode", type=int, default=0)
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
 
 
@@ -310,7 +311,7 @@ def main():
 
     # ---- e2e through the public API: run_statevector + D2H of the final state
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         e2e = run_e2e(lq, qc, gate_bytes, args)
 
     cpu = None

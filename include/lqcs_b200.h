@@ -341,6 +341,44 @@ int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t 
                      int32_t max_fusion_width, int32_t fusion_mode, uint64_t cap,
                      uint32_t* block_width, uint32_t* block_gates, uint64_t* n_blocks);
 
+/* ------------------------------------------------------------------ cost model
+ * A 3-layer, 64-wide FP32 MLP predicting the device time of one device operation from
+ * LQCS_COST_FEATURES features (op kind, width, lowest / highest qubit touched, source gate
+ * count, register size; see lqcs_costmodel_features), trained by the engine's own FP32
+ * forward / backward / Adam kernels on timings the engine measures
+ * (lqcs_program_apply_profiled).  fusion_mode 2 uses it to choose among candidate fusion
+ * plans; without trained weights it falls back to the greedy plan.  Engine extension: no
+ * counterpart in the reference.  Targets are log(milliseconds per 2^24 amplitudes). */
+enum { LQCS_COST_FEATURES = 6, LQCS_COST_HIDDEN = 64 };
+
+/* Feature row of one operation (kind as in lqcs_op_profile, or 6 for a tile pass). */
+int lqcs_costmodel_features(uint32_t kind, uint32_t width, uint32_t min_target,
+                            uint32_t max_target, uint32_t n_gates, uint32_t n_qubits,
+                            float* out);
+
+/* Train from scratch on n rows (features n x LQCS_COST_FEATURES, targets n); the weights
+ * stay in the library.  loss_out (may be NULL) receives the final mean squared error. */
+int lqcs_costmodel_train(const float* features, const float* targets, uint64_t n,
+                         uint32_t epochs, float learning_rate, uint64_t seed, float* loss_out);
+
+/* Predictions for n rows with the current weights. */
+int lqcs_costmodel_predict(const float* features, uint64_t n, float* out);
+
+/* Loss and the flattened gradient of every parameter (W1, b1, W2, b2, W3, b3) on a batch,
+ * without updating; *n_params_out receives the parameter count. */
+int lqcs_costmodel_grad(const float* features, const float* targets, uint64_t n,
+                        float* loss_out, float* grad_out, uint64_t grad_cap,
+                        uint64_t* n_params_out);
+
+/* Get / set / drop the flattened weights. */
+int lqcs_costmodel_get_weights(float* out, uint64_t cap, uint64_t* n_out);
+int lqcs_costmodel_set_weights(const float* w, uint64_t n);
+int lqcs_costmodel_clear(void);
+
+/* Predicted device time (ms) of the plan a fusion mode would build for a circuit. */
+int lqcs_costmodel_plan_ms(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                           int32_t max_fusion_width, int32_t fusion_mode, double* ms_out);
+
 /* ------------------------------------------------------------------ random numbers */
 
 /* `count` draws of lqcs::Rng(seed).uniform() (include/lqcs/core/random.hpp:10-23):

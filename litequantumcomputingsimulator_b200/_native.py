@@ -98,7 +98,7 @@ class OpProfile(C.Structure):
 
 
 OP_KIND_NAMES = {0: "k_apply_1q", 1: "k_phase", 2: "k_dense", 3: "k_diag", 4: "k_perm",
-                 5: "k_pauli"}
+                 5: "k_pauli", 6: "k_tile"}
 
 StatePtr = C.c_void_p
 ProgramPtr = C.c_void_p
@@ -148,6 +148,18 @@ SIGNATURES = {
     "lqcs_fusion_plan": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32, C.c_int32,
                                    C.c_uint64, C.c_void_p, C.c_void_p, _P(C.c_uint64)]),
     "lqcs_rng_uniforms": (C.c_int, [C.c_uint64, C.c_uint64, C.c_void_p]),
+    "lqcs_costmodel_features": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_uint32, C.c_uint32, C.c_void_p]),
+    "lqcs_costmodel_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_float,
+                                       C.c_uint64, _P(C.c_float)]),
+    "lqcs_costmodel_predict": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    "lqcs_costmodel_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, _P(C.c_float), C.c_void_p,
+                                      C.c_uint64, _P(C.c_uint64)]),
+    "lqcs_costmodel_get_weights": (C.c_int, [C.c_void_p, C.c_uint64, _P(C.c_uint64)]),
+    "lqcs_costmodel_set_weights": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "lqcs_costmodel_clear": (C.c_int, []),
+    "lqcs_costmodel_plan_ms": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32,
+                                         C.c_int32, _P(C.c_double)]),
     "lqcs_program_create": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32, C.c_int32,
                                       C.c_int32, _P(ProgramPtr)]),
     "lqcs_program_destroy": (C.c_int, [ProgramPtr]),

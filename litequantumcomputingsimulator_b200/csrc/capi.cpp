@@ -7,6 +7,7 @@
 #include <new>
 #include <string>
 
+#include "costmodel.hpp"
 #include "engine.hpp"
 
 namespace {
@@ -398,6 +399,83 @@ int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonia
     });
 }
 
+int lqcs_costmodel_features(uint32_t kind, uint32_t width, uint32_t min_target,
+                            uint32_t max_target, uint32_t n_gates, uint32_t n_qubits,
+                            float* out) {
+    return guarded([&] {
+        need(out, "out");
+        const auto f = lqcs_b200::op_features(kind, width, min_target, max_target, n_gates, n_qubits);
+        for (int i = 0; i < lqcs_b200::kCostFeatures; ++i) out[i] = f[i];
+    });
+}
+
+int lqcs_costmodel_train(const float* features, const float* targets, uint64_t n,
+                         uint32_t epochs, float learning_rate, uint64_t seed, float* loss_out) {
+    return guarded([&] {
+        need(features, "features");
+        need(targets, "targets");
+        const float loss = lqcs_b200::costmodel_train(features, targets, n, epochs, learning_rate, seed);
+        if (loss_out) *loss_out = loss;
+    });
+}
+
+int lqcs_costmodel_predict(const float* features, uint64_t n, float* out) {
+    return guarded([&] {
+        if (n > 0) {
+            need(features, "features");
+            need(out, "out");
+        }
+        lqcs_b200::costmodel_predict(features, n, out);
+    });
+}
+
+int lqcs_costmodel_grad(const float* features, const float* targets, uint64_t n,
+                        float* loss_out, float* grad_out, uint64_t grad_cap,
+                        uint64_t* n_params_out) {
+    return guarded([&] {
+        need(features, "features");
+        need(targets, "targets");
+        if (n_params_out) *n_params_out = lqcs_b200::kCostParams;
+        if (grad_cap < static_cast<uint64_t>(lqcs_b200::kCostParams))
+            lqcs_b200::invalid("costmodel_grad: gradient buffer too small");
+        need(grad_out, "grad_out");
+        const float loss = lqcs_b200::costmodel_grad(features, targets, n, grad_out);
+        if (loss_out) *loss_out = loss;
+    });
+}
+
+int lqcs_costmodel_get_weights(float* out, uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        const std::vector<float> w = lqcs_b200::costmodel_weights();
+        if (n_out) *n_out = w.size();
+        if (out == nullptr) return;
+        if (cap < w.size()) lqcs_b200::invalid("costmodel_get_weights: buffer too small");
+        std::copy(w.begin(), w.end(), out);
+    });
+}
+
+int lqcs_costmodel_set_weights(const float* w, uint64_t n) {
+    return guarded([&] {
+        need(w, "weights");
+        lqcs_b200::costmodel_set_weights(w, n);
+    });
+}
+
+int lqcs_costmodel_clear(void) {
+    return guarded([&] { lqcs_b200::costmodel_clear(); });
+}
+
+int lqcs_costmodel_plan_ms(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                           int32_t max_fusion_width, int32_t fusion_mode, double* ms_out) {
+    return guarded([&] {
+        need(ms_out, "ms_out");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        auto prog = lqcs_b200::program_create(n_qubits, gates,
+                                              fusion_of(1, max_fusion_width, fusion_mode));
+        *ms_out = lqcs_b200::predict_ops_ms(prog->prog.ops, n_qubits);
+    });
+}
+
 int lqcs_rng_uniforms(uint64_t seed, uint64_t count, double* out) {
     return guarded([&] {
         if (count > 0) need(out, "out");
@@ -412,6 +490,20 @@ int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t 
     return guarded([&] {
         need(n_blocks, "n_blocks");
         const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        if (fusion_mode == lqcs_b200::kFuseTile) {
+            // passes: width = number of high tile qubits, gates = gates applied by the pass
+            const auto items = lqcs_b200::plan_tiles(gates, n_qubits,
+                                                     lqcs_b200::default_tile_config(n_qubits));
+            *n_blocks = items.size();
+            for (uint64_t i = 0; i < items.size() && i < cap; ++i) {
+                const bool pass = items[i].is_pass;
+                if (block_width)
+                    block_width[i] = pass ? static_cast<uint32_t>(items[i].hbits.size())
+                                          : gates[items[i].gate].base_qubits();
+                if (block_gates) block_gates[i] = pass ? static_cast<uint32_t>(items[i].gates.size()) : 1;
+            }
+            return;
+        }
         const auto p = lqcs_b200::plan(gates, n_qubits, fusion_of(1, max_fusion_width, fusion_mode));
         *n_blocks = p.size();
         for (uint64_t i = 0; i < p.size() && i < cap; ++i) {

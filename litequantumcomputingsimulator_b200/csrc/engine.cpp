@@ -1,6 +1,8 @@
 // engine.cpp — device runtime: state handles, programs, run paths, expectations.
 #include "engine.hpp"
 
+#include "costmodel.hpp"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -106,6 +108,20 @@ void Program::build(std::vector<DevOp> ops_in, cudaStream_t stream) {
                                    cudaMemcpyHostToDevice, stream),
                    "upload permutation cycles");
     }
+    std::vector<double2> tmats;
+    for (const cd& z : tile_mats) tmats.push_back(to_d2(z));
+    if (!tile_ops.empty()) {
+        d_tile_ops.ensure(tile_ops.size() * sizeof(TileOp));
+        cuda_check(cudaMemcpyAsync(d_tile_ops.ptr, tile_ops.data(), tile_ops.size() * sizeof(TileOp),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload tile operations");
+    }
+    if (!tmats.empty()) {
+        d_tile_mats.ensure(tmats.size() * sizeof(double2));
+        cuda_check(cudaMemcpyAsync(d_tile_mats.ptr, tmats.data(), tmats.size() * sizeof(double2),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload tile matrices");
+    }
     // the host vectors die with this scope: make sure the copies have consumed them
     cuda_check(cudaStreamSynchronize(stream), "program upload");
 }
@@ -145,6 +161,11 @@ void Program::launch_op(size_t i, const LaunchCtx& ctx, double2* st, uint32_t n,
         case OpKind::PAULI:
             launch_pauli_rotation(ctx, st, n, batch, op.x, op.zy, op.n_y, op.cos_h, op.sin_h);
             break;
+        case OpKind::TILE:
+            launch_tile_pass(ctx, st, n, batch, passes[op.pass_index],
+                             d_tile_ops.as<TileOp>() + pass_op_off[op.pass_index],
+                             d_tile_mats.as<double2>());
+            break;
     }
 }
 
@@ -182,16 +203,105 @@ std::vector<FusedBlock> plan(const std::vector<GateDesc>& gates, uint32_t n,
     return out;
 }
 
+static bool use_tiles(uint32_t n, const FusionConfig& fc) {
+    if (!fc.fuse) return false;
+    if (fc.mode == kFuseTile) return n >= 6;
+    if (fc.mode == kFuseDefault) return n >= 12 && !std::getenv("LQCS_NO_TILES");
+    return false;
+}
+
+// Host side of a tile-pass program (ops not yet uploaded).
+static Program assemble_tiles(const std::vector<GateDesc>& gates, uint32_t n,
+                              const TileConfig& cfg, std::vector<DevOp>& ops) {
+    Program p;
+    for (const PlanItem& it : plan_tiles(gates, n, cfg)) {
+        if (!it.is_pass) {
+            ops.push_back(lower_gate(gates[it.gate], n));
+            continue;
+        }
+        TilePass tp;
+        p.pass_op_off.push_back(p.tile_ops.size());
+        lower_pass(it, gates, cfg, tp, p.tile_ops, p.tile_mats);
+        DevOp op;
+        op.kind = OpKind::TILE;
+        op.k = tp.h;
+        op.targets = it.hbits;
+        op.pass_index = static_cast<uint32_t>(p.passes.size());
+        op.src_gates = static_cast<uint32_t>(it.gates.size());
+        op.alg_fraction = 1.0;
+        p.passes.push_back(tp);
+        ops.push_back(std::move(op));
+    }
+    return p;
+}
+
+static std::vector<DevOp> dense_ops(const std::vector<GateDesc>& gates, uint32_t n, uint32_t width) {
+    FusionConfig g;
+    g.fuse = true;
+    g.max_width = width;
+    g.mode = kFuseGreedy;
+    return lower_plan(plan(gates, n, g), gates, n);
+}
+
+// Learned planning: every candidate plan (greedy dense blocks of width 1..6, tile passes of
+// several shapes) is scored by the cost model's predicted device time; the cheapest wins.
+// Without trained weights the plain greedy plan is used.
+static Program compile_learned(const std::vector<GateDesc>& gates, uint32_t n,
+                               const FusionConfig& fc, cudaStream_t stream) {
+    if (!costmodel_trained()) {
+        Program p;
+        p.build(dense_ops(gates, n, fc.max_width ? fc.max_width : default_fusion_width()), stream);
+        return p;
+    }
+    double best = -1.0;
+    Program best_prog;
+    std::vector<DevOp> best_ops;
+    for (uint32_t w = 1; w <= kMaxDense && w <= n; ++w) {
+        std::vector<DevOp> ops = dense_ops(gates, n, w);
+        const double ms = predict_ops_ms(ops, n);
+        if (best < 0 || ms < best) {
+            best = ms;
+            best_prog = Program();
+            best_ops = std::move(ops);
+        }
+    }
+    if (n >= 6) {
+        const uint32_t shapes[][3] = {{11, 5, 2}, {12, 5, 2}, {12, 5, 3}, {13, 5, 2}, {13, 5, 3}};
+        for (const auto& s : shapes) {
+            TileConfig cfg;
+            cfg.m = std::min<uint32_t>(s[0], n);
+            cfg.L = std::min<uint32_t>(s[1], cfg.m);
+            cfg.inner = s[2];
+            std::vector<DevOp> ops;
+            Program p = assemble_tiles(gates, n, cfg, ops);
+            const double ms = predict_ops_ms(ops, n);
+            if (ms < best) {
+                best = ms;
+                best_prog = std::move(p);
+                best_ops = std::move(ops);
+            }
+        }
+    }
+    best_prog.build(std::move(best_ops), stream);
+    return best_prog;
+}
+
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
                 cudaStream_t stream) {
+    if (fc.fuse && fc.mode == kFuseLearned) return compile_learned(gates, n, fc, stream);
     std::vector<DevOp> ops;
-    if (fc.fuse && fc.mode != 3) {
+    if (use_tiles(n, fc)) {
+        Program p = assemble_tiles(gates, n, default_tile_config(n), ops);
+        p.build(std::move(ops), stream);
+        return p;
+    }
+    Program p;
+    if (fc.fuse && fc.mode != kFuseNone) {
         ops = lower_plan(plan(gates, n, fc), gates, n);
     } else {
         for (const GateDesc& g : gates)
             if (g.is_unitary()) ops.push_back(lower_gate(g, n));
     }
-    Program p;
     p.build(std::move(ops), stream);
     return p;
 }
@@ -449,63 +559,6 @@ std::vector<Channel> decode_channels(const lqcs_sim_options* opts) {
     return out;
 }
 
-// Apply an arbitrary 2x2 to qubit q of state 0.
-void apply_matrix_1q(lqcs_state& st, uint32_t q, const Kraus& m, DeviceBuffer& tmp) {
-    if (st.n >= 5) {
-        Apply1QOp a{};
-        for (int e = 0; e < 4; ++e) a.m[e] = to_d2(m[e]);
-        a.t = q;
-        a.cmask = 0;
-        a.diag = (m[1] == cd{0, 0} && m[2] == cd{0, 0}) ? 1 : 0;
-        launch_apply_1q(st.ctx, st.d(), st.n, 1, a);
-        return;
-    }
-    tmp.ensure(4 * sizeof(double2));
-    const double2 h[4] = {to_d2(m[0]), to_d2(m[1]), to_d2(m[2]), to_d2(m[3])};
-    cuda_check(cudaMemcpyAsync(tmp.ptr, h, sizeof(h), cudaMemcpyHostToDevice, st.stream), "H2D");
-    launch_dense(st.ctx, st.d(), st.n, 1, &q, 1, 0, tmp.as<double2>());
-    st.sync();
-}
-
-// sample_kraus_branch (src/backend/statevector_simulator.cpp:122-144): one uniform, branch
-// probabilities ||K_i psi||^2 (here all from one reduced density matrix of qubit q),
-// skip p <= 0, choose the first i with u < cumulative p, fall back to the last non-zero
-// branch, apply K_i / sqrt(p_i).
-void sample_kraus_branch(lqcs_state& st, const Channel& ch, uint32_t q, double u,
-                         DeviceBuffer& tmp) {
-    double* part = st.partials(4);
-    double* out = part + (kMaxReduceBlocks + 1) * 4;
-    launch_rdm1(st.ctx, st.d(), st.n, q, part, out);
-    double r[4];
-    cuda_check(cudaMemcpyAsync(r, out, sizeof(r), cudaMemcpyDeviceToHost, st.stream), "D2H rdm");
-    st.sync();
-    const cd rho00{r[0], 0.0}, rho11{r[1], 0.0}, rho01{r[2], r[3]}, rho10 = std::conj(rho01);
-    double cum = 0.0;
-    int chosen = -1;
-    double chosen_p = 0.0;
-    for (size_t i = 0; i < ch.size(); ++i) {
-        const Kraus& k = ch[i];
-        // Tr(K rho K^dagger) = sum_r sum_{c,c'} K[r][c] rho[c][c'] conj(K[r][c'])
-        cd p{0.0, 0.0};
-        for (int row = 0; row < 2; ++row) {
-            const cd k0 = k[2 * row], k1 = k[2 * row + 1];
-            p += k0 * rho00 * std::conj(k0) + k0 * rho01 * std::conj(k1) +
-                 k1 * rho10 * std::conj(k0) + k1 * rho11 * std::conj(k1);
-        }
-        const double pr = p.real();
-        if (pr <= 0.0) continue;
-        chosen = static_cast<int>(i);
-        chosen_p = pr;
-        cum += pr;
-        if (u < cum) break;
-    }
-    if (chosen < 0) return;
-    const double inv = 1.0 / std::sqrt(chosen_p);
-    const Kraus& k = ch[chosen];
-    const Kraus m{k[0] * inv, k[1] * inv, k[2] * inv, k[3] * inv};
-    apply_matrix_1q(st, q, m, tmp);
-}
-
 // Emission order of SingleQubitGateFusion (src/transpiler/gate_fusion.cpp:32-67), reduced
 // to what run()'s path selection reads from it: true when some unitary is emitted after a
 // Measure.  Pending one-qubit products are flushed on any other instruction touching the
@@ -589,10 +642,9 @@ void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates
         fc.max_width = static_cast<uint32_t>(std::max(0, opts->max_fusion_width));
         fc.mode = opts->fusion_mode;
     }
-    auto st = new_state(n, 1, nullptr);
-
     if (!per_shot) {
         // run_sampling (src/backend/statevector_simulator.cpp:88-119)
+        auto st = new_state(n, 1, nullptr);
         apply_circuit(*st, gates, fc);
         std::vector<int64_t> src(n_clbits, -1);
         for (const GateDesc& g : gates)
@@ -610,77 +662,11 @@ void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates
         return;
     }
 
-    // run_per_shot (src/backend/statevector_simulator.cpp:156-190): compile the unitary
-    // stretches between non-unitary instructions once; noisy circuits keep one gate per
-    // stretch because noise follows every gate.
-    struct Item {
-        int kind;          // 0 unitary program, 1 measure, 2 reset, 3 kraus
-        size_t prog = 0;
-        uint32_t q = 0, clbit = 0;
-        std::vector<uint32_t> noise_qubits;
-        Channel kraus;
-    };
-    std::vector<Program> progs;
-    std::vector<Item> items;
-    std::vector<GateDesc> stretch;
-    auto flush_stretch = [&]() {
-        if (stretch.empty()) return;
-        progs.push_back(compile(stretch, n, fc, st->stream));
-        Item it;
-        it.kind = 0;
-        it.prog = progs.size() - 1;
-        items.push_back(std::move(it));
-        stretch.clear();
-    };
-    for (const GateDesc& g : gates) {
-        if (g.type == LQCS_GATE_BARRIER) continue;
-        if (g.type == LQCS_GATE_MEASURE || g.type == LQCS_GATE_RESET || g.type == LQCS_GATE_KRAUS) {
-            flush_stretch();
-            Item it;
-            it.kind = g.type == LQCS_GATE_MEASURE ? 1 : g.type == LQCS_GATE_RESET ? 2 : 3;
-            it.q = g.qubits[0];
-            it.clbit = g.clbit;
-            if (it.kind == 3) it.kraus.assign(g.kraus.begin(), g.kraus.end());
-            items.push_back(std::move(it));
-            continue;
-        }
-        stretch.push_back(g);
-        if (noisy) {
-            flush_stretch();
-            items.back().noise_qubits = g.qubits;
-        }
-    }
-    flush_stretch();
-
-    DeviceBuffer tmp;
-    for (uint64_t s = 0; s < shots; ++s) {
-        launch_set_basis(st->ctx, st->d(), n, 1, 0);
-        uint64_t creg = 0;
-        for (const Item& it : items) {
-            switch (it.kind) {
-                case 0:
-                    progs[it.prog].launch(st->ctx, st->d(), n, 1);
-                    for (const Channel& ch : channels)
-                        for (uint32_t q : it.noise_qubits)
-                            sample_kraus_branch(*st, ch, q, rng_uniform(rng), tmp);
-                    break;
-                case 1: {
-                    const int out = collapse(*st, it.q, rng_uniform(rng));
-                    if (out) creg |= uint64_t{1} << it.clbit;
-                    else creg &= ~(uint64_t{1} << it.clbit);
-                    break;
-                }
-                case 2:
-                    reset_qubit(*st, it.q, rng_uniform(rng));
-                    break;
-                case 3:
-                    sample_kraus_branch(*st, it.kraus, it.q, rng_uniform(rng), tmp);
-                    break;
-            }
-        }
-        regs[s] = creg;
-    }
-    st->sync();
+    // run_per_shot (src/backend/statevector_simulator.cpp:156-190), many shots at a time
+    std::vector<std::vector<std::array<cd, 4>>> chans;
+    for (const Channel& c : channels) chans.emplace_back(c.begin(), c.end());
+    const uint32_t resident = opts ? static_cast<uint32_t>(std::max(0, opts->max_resident)) : 0;
+    run_per_shot_batched(n, gates, shots, chans, fc, rng, resident, regs);
 }
 
 // ------------------------------------------------------------------ Hamiltonians

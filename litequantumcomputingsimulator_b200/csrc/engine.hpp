@@ -10,6 +10,7 @@
 
 #include "gates.hpp"
 #include "kernels.cuh"
+#include "tile_plan.hpp"
 
 namespace lqcs_b200 {
 
@@ -50,6 +51,12 @@ struct Program {
     std::vector<uint64_t> len_off;   // per op: offset (uint32) of its cycle lengths
     DeviceBuffer d_mats, d_u32;
     uint64_t source_gates = 0;
+    // shared-memory tile passes (ops of kind TILE index into these)
+    std::vector<TilePass> passes;
+    std::vector<uint64_t> pass_op_off;   // first TileOp of each pass
+    std::vector<TileOp> tile_ops;
+    std::vector<cd> tile_mats;
+    DeviceBuffer d_tile_ops, d_tile_mats;
 
     void build(std::vector<DevOp> ops_in, cudaStream_t stream);
     void launch(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch) const;
@@ -60,8 +67,9 @@ struct Program {
 struct FusionConfig {
     bool fuse = true;
     uint32_t max_width = 0;   // 0 = engine default
-    int mode = 0;             // 0 default, 1 greedy, 2 learned, 3 none
+    int mode = 0;             // 0 default, 1 greedy dense blocks, 2 learned, 3 none, 4 tile passes
 };
+enum FusionMode { kFuseDefault = 0, kFuseGreedy = 1, kFuseLearned = 2, kFuseNone = 3, kFuseTile = 4 };
 uint32_t default_fusion_width();
 
 // Compile a list of unitary gates to a Program (fused or gate by gate).
@@ -125,6 +133,13 @@ void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, doub
 uint32_t static_expectation_max_terms();
 void expectation_terms_static(const void* d_amps, uint32_t n_qubits, const char* const* paulis,
                               uint64_t n_terms, double* host_values, cudaStream_t stream);
+
+// Per-shot evolution (mid-circuit measurement, reset, noise) with many shots resident on
+// the device (trajectory.cpp).  `regs` receives the classical register of every shot.
+void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64_t shots,
+                          const std::vector<std::vector<std::array<cd, 4>>>& channels,
+                          const FusionConfig& fc, Rng& rng, uint32_t max_resident,
+                          uint64_t* regs);
 
 // StatevectorSimulator::run.
 void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,

@@ -566,9 +566,7 @@ std::vector<DevOp> lower_plan(const std::vector<FusedBlock>& plan,
         op.k = k;
         op.targets = b.qubits;
         op.src_gates = static_cast<uint32_t>(b.gates.size());
-        double f = 0.0;
-        for (uint32_t gi : b.gates) f = std::max(f, gate_alg_fraction(gates[gi]));
-        op.alg_fraction = f;
+        op.alg_fraction = 1.0;   // a fused block reads and writes every amplitude
         const bool diag = is_diag_matrix(m, dim);
         if (k == 1 && n >= 5) {
             if (diag && m[0] == cd{1.0, 0.0}) {

@@ -66,7 +66,7 @@ std::vector<GateDesc> decode_all(const lqcs_instruction* insts, uint64_t n_insts
                                  uint32_t n_qubits);
 
 // ------------------------------------------------------------------ device operations
-enum class OpKind { K1Q, PHASE, DENSE, DIAG, PERM, PAULI };
+enum class OpKind { K1Q, PHASE, DENSE, DIAG, PERM, PAULI, TILE };
 
 struct DevOp {
     OpKind kind = OpKind::DENSE;
@@ -87,6 +87,8 @@ struct DevOp {
     uint64_t x = 0, zy = 0;
     uint32_t n_y = 0;
     double cos_h = 1.0, sin_h = 0.0;
+    // TILE: index of the shared-memory pass in the program
+    uint32_t pass_index = 0;
     // bookkeeping
     uint32_t src_gates = 1;              // source gates merged into this op
     double alg_fraction = 1.0;           // fraction of amplitudes it can change

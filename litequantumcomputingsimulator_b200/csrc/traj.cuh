@@ -1,0 +1,43 @@
+// traj.cuh — batched trajectory kernels (traj_kernels.cu).
+#pragma once
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace lqcs_b200 {
+
+constexpr uint32_t kTrajMaxBlocks = 64;   // reduction blocks per state
+
+struct TrajDecide {
+    int mode;                 // 0 Kraus branch, 1 Born-rule outcome (measure / reset)
+    int is_measure;           // mode 1: record the outcome in the classical register
+    uint32_t clbit;
+    uint32_t uniform_index;   // index of this event's uniform within a shot
+    uint32_t n_ops;           // mode 0: Kraus operators (2x2 each, device memory)
+    const double2* ops;
+};
+
+// Device scratch for a resident batch of R trajectories.
+struct TrajScratch {
+    double* partials;   // R * 4 * kTrajMaxBlocks
+    double2* mats;      // R * 4
+    int* flag;          // R
+    double* scale;      // R
+    uint64_t* regs;     // R classical registers
+};
+
+// rdm of qubit q per state -> branch per state (uniform u[(first+b)*per_shot+j]) ->
+// K/sqrt(p) applied per state.
+void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
+                       const TrajDecide& d, const double* d_uniforms, uint64_t first,
+                       uint64_t per_shot, TrajScratch& s);
+// Born-rule collapse (reset = 0) or reset to |0> (reset = 1) per state.
+void launch_traj_measure(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
+                         uint32_t q, const TrajDecide& d, const double* d_uniforms,
+                         uint64_t first, uint64_t per_shot, int reset, TrajScratch& s);
+// Per-state choice into a table of normalised 2x2 operators (choice < 0: no-op).
+void launch_traj_table(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
+                       const double2* d_mats, const int* d_choice);
+
+}  // namespace lqcs_b200

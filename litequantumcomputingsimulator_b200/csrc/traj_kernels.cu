@@ -1,0 +1,253 @@
+// traj_kernels.cu — batched per-shot evolution: many trajectories resident at once.
+//
+// The reference evolves shots one after another (run_per_shot,
+// src/backend/statevector_simulator.cpp:156-190): per Measure a collapse
+// (gate_kernels.cpp:227-247), per Reset a reset (:249-260), per noise point one uniform,
+// a branch probability ||K_i psi||^2 per Kraus operator and K_i/sqrt(p_i) applied
+// (statevector_simulator.cpp:122-144).  Here R trajectories advance together: state b of a
+// batch is trajectory `first + b`; every random decision of trajectory t reads its own
+// uniform u[t * per_shot + j], so decisions stay per trajectory while each kernel walks the
+// whole batch.  No host round trip happens inside a batch.
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+
+#include "traj.cuh"
+
+namespace lqcs_b200 {
+
+namespace {
+
+void check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string("CUDA launch failed in ") + what + ": " +
+                                 cudaGetErrorString(e));
+    }
+    count_launch();
+}
+
+constexpr uint32_t kThreads = 256;
+
+uint32_t blocks_per_state(const LaunchCtx& ctx, uint64_t work, uint32_t batch) {
+    const uint64_t want = (work + kThreads - 1) / kThreads;
+    const uint64_t cap = std::max<uint64_t>(1, static_cast<uint64_t>(ctx.num_sms) * 8 /
+                                                   std::max(1u, batch));
+    return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>({want, cap,
+                                                                           kTrajMaxBlocks})));
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* out_row, uint32_t stride) {
+    __shared__ double sh[NV][kThreads / 32];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = 0.0;
+        for (int w = 0; w < static_cast<int>(kThreads / 32); ++w) t += sh[threadIdx.x][w];
+        out_row[threadIdx.x * stride] = t;
+    }
+}
+
+// Per state: rho of qubit q = {sum |a0|^2, sum |a1|^2, Re sum a0 conj(a1), Im ...}
+// partials layout [state][value][block]
+__global__ void __launch_bounds__(kThreads) k_b_rdm1(const double2* __restrict__ st, uint64_t len,
+                                                     uint32_t q, double* __restrict__ partials) {
+    const double2* s = st + static_cast<uint64_t>(blockIdx.y) * len;
+    const uint64_t half = len >> 1, qb = uint64_t{1} << q;
+    double v[4] = {0, 0, 0, 0};
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < half;
+         g += stride) {
+        const uint64_t i0 = insert_zero_bit(g, q);
+        const double2 a0 = __ldg(s + i0), a1 = __ldg(s + (i0 | qb));
+        v[0] += a0.x * a0.x + a0.y * a0.y;
+        v[1] += a1.x * a1.x + a1.y * a1.y;
+        v[2] += a0.x * a1.x + a0.y * a1.y;
+        v[3] += a0.y * a1.x - a0.x * a1.y;
+    }
+    block_sum<4>(v, partials + static_cast<uint64_t>(blockIdx.y) * 4 * gridDim.x + blockIdx.x,
+                 gridDim.x);
+}
+
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// One thread per state: sum the partials, then decide.
+// mode 0 (Kraus): probabilities Tr(K_i rho K_i^dagger), first i with u < cumulative p
+//                 (p <= 0 skipped, last non-zero branch as fallback), mats[b] = K_i/sqrt(p_i),
+//                 flag[b] = 1 (0 only when every probability is zero: nothing is applied).
+// mode 1 (measure/reset): p1 = rho11, outcome = u < p1, scale 1/sqrt(keep); the clbit of
+//                 the register is set or cleared (measure only).
+__global__ void k_b_decide(const double* __restrict__ partials, uint32_t nb, uint32_t batch,
+                           TrajDecide d, const double* __restrict__ uniforms, uint64_t first,
+                           uint64_t per_shot, double2* __restrict__ mats, int* __restrict__ flag,
+                           double* __restrict__ scale, uint64_t* __restrict__ regs) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    double r[4] = {0, 0, 0, 0};
+    const double* row = partials + static_cast<uint64_t>(b) * 4 * nb;
+    for (int k = 0; k < 4; ++k)
+        for (uint32_t j = 0; j < nb; ++j) r[k] += row[k * nb + j];
+    const double u = uniforms[(first + b) * per_shot + d.uniform_index];
+    if (d.mode == 1) {
+        const double p1 = r[1];
+        const int outcome = u < p1 ? 1 : 0;
+        const double keep = outcome ? p1 : 1.0 - p1;
+        flag[b] = outcome;
+        scale[b] = 1.0 / sqrt(keep);
+        if (d.is_measure) {
+            const uint64_t bit = uint64_t{1} << d.clbit;
+            regs[b] = outcome ? (regs[b] | bit) : (regs[b] & ~bit);
+        }
+        return;
+    }
+    const double2 rho00 = make_double2(r[0], 0.0), rho11 = make_double2(r[1], 0.0);
+    const double2 rho01 = make_double2(r[2], r[3]), rho10 = make_double2(r[2], -r[3]);
+    double cum = 0.0, chosen_p = 0.0;
+    int chosen = -1;
+    for (uint32_t i = 0; i < d.n_ops; ++i) {
+        const double2* k = d.ops + 4 * i;
+        double2 p = make_double2(0.0, 0.0);
+        for (int row2 = 0; row2 < 2; ++row2) {
+            const double2 k0 = k[2 * row2], k1 = k[2 * row2 + 1];
+            p = cadd(p, cmul(cmul(k0, rho00), cconj(k0)));
+            p = cadd(p, cmul(cmul(k0, rho01), cconj(k1)));
+            p = cadd(p, cmul(cmul(k1, rho10), cconj(k0)));
+            p = cadd(p, cmul(cmul(k1, rho11), cconj(k1)));
+        }
+        if (p.x <= 0.0) continue;
+        chosen = static_cast<int>(i);
+        chosen_p = p.x;
+        cum += p.x;
+        if (u < cum) break;
+    }
+    if (chosen < 0) {
+        flag[b] = 0;
+        return;
+    }
+    const double inv = 1.0 / sqrt(chosen_p);
+    const double2* k = d.ops + 4 * chosen;
+    for (int e = 0; e < 4; ++e) mats[4 * b + e] = cscale(k[e], inv);
+    flag[b] = 1;
+}
+
+// Per-state 2x2 on qubit q (state b uses mats[4b..4b+3]); skipped where flag[b] == 0.
+__global__ void __launch_bounds__(kThreads) k_b_apply_mats(double2* __restrict__ st, uint64_t len,
+                                                           uint32_t q, const double2* __restrict__ mats,
+                                                           const int* __restrict__ flag) {
+    const uint32_t b = blockIdx.y;
+    if (flag[b] == 0) return;
+    double2* s = st + static_cast<uint64_t>(b) * len;
+    const double2 m0 = mats[4 * b], m1 = mats[4 * b + 1], m2 = mats[4 * b + 2], m3 = mats[4 * b + 3];
+    const uint64_t half = len >> 1, qb = uint64_t{1} << q;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < half;
+         g += stride) {
+        const uint64_t i0 = insert_zero_bit(g, q);
+        const double2 a0 = s[i0], a1 = s[i0 | qb];
+        s[i0] = cmad(m1, a1, cmul(m0, a0));
+        s[i0 | qb] = cmad(m3, a1, cmul(m2, a0));
+    }
+}
+
+// Collapse: keep bit q == outcome[b] scaled by scale[b]; with `reset`, a 1 outcome is then
+// moved back to |0> (kernels::reset_qubit).
+__global__ void __launch_bounds__(kThreads) k_b_project(double2* __restrict__ st, uint64_t len,
+                                                        uint32_t q, const int* __restrict__ outcome,
+                                                        const double* __restrict__ scale, int reset) {
+    const uint32_t b = blockIdx.y;
+    double2* s = st + static_cast<uint64_t>(b) * len;
+    const int o = outcome[b];
+    const double sc = scale[b];
+    const uint64_t half = len >> 1, qb = uint64_t{1} << q;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < half;
+         g += stride) {
+        const uint64_t i0 = insert_zero_bit(g, q);
+        const double2 a0 = s[i0], a1 = s[i0 | qb];
+        const double2 z = make_double2(0.0, 0.0);
+        if (o == 0) {
+            s[i0] = cscale(a0, sc);
+            s[i0 | qb] = z;
+        } else if (reset) {
+            s[i0] = cscale(a1, sc);
+            s[i0 | qb] = z;
+        } else {
+            s[i0] = z;
+            s[i0 | qb] = cscale(a1, sc);
+        }
+    }
+}
+
+// Unitary-mixture channels (every K_i proportional to a unitary): the branch does not
+// depend on the state, so it is chosen for every trajectory of the whole run up front on
+// the host; here each state applies its own (possibly identity-skipped) 2x2.
+__global__ void __launch_bounds__(kThreads) k_b_apply_table(double2* __restrict__ st, uint64_t len,
+                                                            uint32_t q, const double2* __restrict__ mats,
+                                                            const int* __restrict__ choice) {
+    const uint32_t b = blockIdx.y;
+    const int c = choice[b];
+    if (c < 0) return;
+    double2* s = st + static_cast<uint64_t>(b) * len;
+    const double2 m0 = mats[4 * c], m1 = mats[4 * c + 1], m2 = mats[4 * c + 2], m3 = mats[4 * c + 3];
+    const uint64_t half = len >> 1, qb = uint64_t{1} << q;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < half;
+         g += stride) {
+        const uint64_t i0 = insert_zero_bit(g, q);
+        const double2 a0 = s[i0], a1 = s[i0 | qb];
+        s[i0] = cmad(m1, a1, cmul(m0, a0));
+        s[i0 | qb] = cmad(m3, a1, cmul(m2, a0));
+    }
+}
+
+}  // namespace
+
+void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
+                       const TrajDecide& d, const double* d_uniforms, uint64_t first,
+                       uint64_t per_shot, TrajScratch& s) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
+    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials);
+    check_launch("traj_rdm1");
+    k_b_decide<<<(batch + 127) / 128, 128, 0, ctx.stream>>>(s.partials, nb, batch, d, d_uniforms,
+                                                             first, per_shot, s.mats, s.flag,
+                                                             s.scale, s.regs);
+    check_launch("traj_decide");
+    k_b_apply_mats<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.mats, s.flag);
+    check_launch("traj_apply");
+}
+
+void launch_traj_measure(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
+                         uint32_t q, const TrajDecide& d, const double* d_uniforms,
+                         uint64_t first, uint64_t per_shot, int reset, TrajScratch& s) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
+    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials);
+    check_launch("traj_rdm1");
+    k_b_decide<<<(batch + 127) / 128, 128, 0, ctx.stream>>>(s.partials, nb, batch, d, d_uniforms,
+                                                             first, per_shot, s.mats, s.flag,
+                                                             s.scale, s.regs);
+    check_launch("traj_decide");
+    k_b_project<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.flag, s.scale, reset);
+    check_launch("traj_project");
+}
+
+void launch_traj_table(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
+                       const double2* d_mats, const int* d_choice) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
+    k_b_apply_table<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, d_mats, d_choice);
+    check_launch("traj_table");
+}
+
+}  // namespace lqcs_b200

@@ -1,0 +1,44 @@
+"""torch.autograd integration: <psi(theta)|H|psi(theta)> as a differentiable function of the
+parameters of a ParametricCircuit, with the gradient from the engine's batched adjoint
+kernels (one forward and one backward statevector sweep per parameter set) instead of the
+reference's parameter-shift rule (src/algorithms/vqe.cpp:68-94)."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .algorithms import adjoint_gradient
+from .circuit import ParametricCircuit
+
+
+class AdjointExpectation(torch.autograd.Function):
+    """energies = E(params); params is (P,) or (B, P).  The gradient is computed together
+    with the energy in forward() and reused by backward()."""
+
+    @staticmethod
+    def forward(ctx, params: torch.Tensor, ansatz: ParametricCircuit, hamiltonian,
+                max_resident: int = 0):
+        p = params.detach().to("cpu", torch.float64).numpy()
+        single = p.ndim == 1
+        e, g = adjoint_gradient(hamiltonian, ansatz, p.reshape(-1, ansatz.num_parameters()),
+                                max_resident=max_resident)
+        grad = torch.as_tensor(np.asarray(g), dtype=params.dtype, device=params.device)
+        energies = torch.as_tensor(np.asarray(e), dtype=params.dtype, device=params.device)
+        if single:
+            grad = grad.reshape(-1)
+            energies = energies.reshape(())
+        ctx.save_for_backward(grad)
+        return energies
+
+    @staticmethod
+    def backward(ctx, grad_out: torch.Tensor):
+        (grad,) = ctx.saved_tensors
+        if grad_out.dim() == 0:
+            return grad_out * grad, None, None, None
+        return grad_out.unsqueeze(-1) * grad, None, None, None
+
+
+def expectation(params: torch.Tensor, ansatz: ParametricCircuit, hamiltonian,
+                max_resident: int = 0) -> torch.Tensor:
+    """Differentiable <psi(params)|H|psi(params)>; hamiltonian = [(coeff, pauli), ...]."""
+    return AdjointExpectation.apply(params, ansatz, hamiltonian, max_resident)

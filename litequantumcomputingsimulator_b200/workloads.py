@@ -149,6 +149,37 @@ def gaussian_state(n: int, seed: int) -> np.ndarray:
     return out
 
 
+def random_mix_circuit(n: int, depth: int, seed: int) -> QuantumCircuit:
+    """Gate mix of the cost-model workload: per layer, about n gates drawn 50 % U3,
+    30 % CX or CZ (random pair), 10 % RZZ (random pair, random angle), 10 % Pauli
+    rotation of weight 2..8 on random qubits."""
+    rng = UniformStream(seed)
+    qc = QuantumCircuit(n)
+    two_pi = 2.0 * math.pi
+    for _ in range(depth):
+        for _ in range(n):
+            r = rng.next()
+            if r < 0.5:
+                q = rng.randint(n)
+                th, ph, la = (two_pi * v for v in rng.take(3))
+                qc.u(th, ph, la, q)
+            elif r < 0.8:
+                a, b = _shuffle(list(range(n)), rng)[:2]
+                if rng.next() < 0.5:
+                    qc.cx(a, b)
+                else:
+                    qc.cz(a, b)
+            elif r < 0.9:
+                a, b = _shuffle(list(range(n)), rng)[:2]
+                qc.rzz(two_pi * rng.next(), a, b)
+            else:
+                w = 2 + rng.randint(min(8, n) - 1)
+                support = _shuffle(list(range(n)), rng)[:w]
+                pauli = "".join("XYZ"[rng.randint(3)] for _ in range(w))
+                qc.rp(two_pi * rng.next() - math.pi, pauli, support)
+    return qc
+
+
 def alg_bytes(circuit: QuantumCircuit) -> float:
     """Algorithmic bytes of a circuit's gates on its register: sum over gates of
     32 * 2^n * f, f = the fraction of amplitudes the gate can change (dense and fused

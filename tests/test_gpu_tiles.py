@@ -1,0 +1,113 @@
+"""GPU parity of the shared-memory tile passes (fusion_mode 4, the default from 12 qubits)
+and of the greedy dense-block path (fusion_mode 1) against the oracle, for every gate type
+and several tile shapes."""
+import os
+
+import numpy as np
+import pytest
+
+import litequantumcomputingsimulator_b200 as lq
+from litequantumcomputingsimulator_b200 import workloads as W
+
+from helpers import random_circuit
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+TILE = 4
+GREEDY = 1
+
+
+@pytest.fixture
+def tile_env():
+    keys = ("LQCS_TILE_BITS", "LQCS_TILE_LOW", "LQCS_TILE_INNER")
+    saved = {k: os.environ.get(k) for k in keys}
+
+    def set_cfg(m, low, inner):
+        os.environ["LQCS_TILE_BITS"] = str(m)
+        os.environ["LQCS_TILE_LOW"] = str(low)
+        os.environ["LQCS_TILE_INNER"] = str(inner)
+
+    yield set_cfg
+    for k, v in saved.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
+
+
+def run(qc, mode, init=None):
+    if init is None:
+        return lq.StatevectorSimulator(fusion_mode=mode).run_statevector(qc).to_numpy()
+    sv = lq.Statevector.from_numpy(init)
+    sv.apply(qc, fuse_gates=True, fusion_mode=mode)
+    return sv.to_numpy()
+
+
+@pytest.mark.parametrize("n", [6, 8, 11, 13])
+@pytest.mark.parametrize("cfg", [(12, 5, 2), (11, 5, 1), (13, 5, 3), (10, 6, 4), (12, 4, 2)])
+def test_tile_passes_every_gate_type(port, tile_env, n, cfg):
+    tile_env(*cfg)
+    init = W.gaussian_state(n, seed=n + cfg[0])
+    qc = random_circuit(n, 90, seed=31 * n + cfg[2], max_controls=4, max_unitary=4)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    got = run(qc, TILE, init)
+    assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("inner", [1, 2, 3, 4])
+def test_tile_brickwork_and_qft_vs_reference(ref, tile_env, inner):
+    tile_env(12, 5, inner)
+    qc = W.brickwork(18, 12, seed=77)
+    want = ref.run_statevector(qc, fuse=True)
+    assert np.max(np.abs(run(qc, TILE) - want)) < TOL
+    init = W.gaussian_state(16, seed=4)
+    q = lq.algorithms.qft(16)
+    want = ref.evolve_from(q, init)
+    assert np.max(np.abs(run(q, TILE, init) - want)) < TOL
+
+
+def test_tile_barrier_and_wide_gates(port, tile_env):
+    tile_env(12, 5, 2)
+    n = 14
+    init = W.gaussian_state(n, seed=8)
+    qc = random_circuit(n, 40, seed=5)
+    qc.barrier()
+    qc.rp(0.3, "XYZXYZX", [0, 3, 5, 7, 9, 11, 13])    # wider than a tile op: runs on its own
+    qc.mcx([0, 1, 2, 3, 4, 5, 6, 7, 8], 13)             # too many controls for a tile op
+    qc.permutation(list(np.random.default_rng(1).permutation(32)), [1, 6, 8, 10, 12])
+    qc.compose(random_circuit(n, 40, seed=6))
+    want = port.run_statevector(qc, fuse=False, state=init)
+    assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+
+
+@pytest.mark.parametrize("n", [12, 15])
+def test_greedy_blocks_at_tile_sizes(port, n):
+    init = W.gaussian_state(n, seed=n)
+    qc = random_circuit(n, 70, seed=n)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    for width in (2, 4, 6):
+        sv = lq.Statevector.from_numpy(init)
+        sv.apply(qc, fuse_gates=True, max_fusion_width=width, fusion_mode=GREEDY)
+        assert np.max(np.abs(sv.to_numpy() - want)) < TOL
+
+
+def test_tile_batch_of_states(port, tile_env):
+    """Tile passes walk a batch of states (gridDim.y)."""
+    tile_env(12, 5, 2)
+    from litequantumcomputingsimulator_b200 import _native as N
+    import ctypes as C
+    n, batch = 13, 3
+    qc = random_circuit(n, 50, seed=9)
+    inits = [W.gaussian_state(n, seed=s) for s in range(batch)]
+    h = N.StatePtr()
+    N.call("lqcs_state_create_batch", n, batch, None, C.byref(h))
+    flat = np.ascontiguousarray(np.concatenate(inits))
+    N.call("lqcs_state_load", h, flat.ctypes.data, flat.size)
+    prog = lq.simulator.CompiledCircuit(qc, True, 0, TILE)
+    N.call("lqcs_program_apply", h, prog._h)
+    out = np.empty_like(flat)
+    N.call("lqcs_state_store", h, out.ctypes.data, out.size)
+    N.call("lqcs_state_destroy", h)
+    for b in range(batch):
+        want = port.run_statevector(qc, fuse=False, state=inits[b])
+        assert np.max(np.abs(out[b << n:(b + 1) << n] - want)) < TOL

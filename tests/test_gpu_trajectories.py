@@ -1,0 +1,68 @@
+"""Batched trajectories (per-shot path with many shots resident on the device).
+
+* Same seed, same uniforms: counts identical to the reference's per-shot semantics
+  (oracle/_ref: StatevectorSimulator::run for a noise model, the reference-semantics
+  driver for explicit Kraus placements).
+* The config-3 cross-check: a 10-qubit noisy brickwork (depolarizing 1e-3 after U3,
+  1e-2 on both qubits after CX, amplitude damping 1e-3 per qubit per layer), 1024
+  trajectories, total-variation distance to the exact density-matrix distribution compared
+  with the TVD of 1024 independent draws from that distribution (seeded bootstrap).
+"""
+import numpy as np
+import pytest
+
+import litequantumcomputingsimulator_b200 as lq
+from litequantumcomputingsimulator_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def counts_of(regs):
+    vals, cnt = np.unique(regs, return_counts=True)
+    return {int(v): int(c) for v, c in zip(vals, cnt)}
+
+
+@pytest.mark.parametrize("resident", [1, 7, 64])
+def test_noise_model_counts_identical(ref, resident):
+    noise = lq.NoiseModel()
+    noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.2))
+    noise.add_all_qubit_channel(lq.KrausChannel.amplitude_damping(0.15))
+    noise.add_all_qubit_channel(lq.KrausChannel.phase_flip(0.1))
+    qc = lq.QuantumCircuit(5, 5)
+    qc.h(0).cx(0, 1).ry(0.7, 2).cx(2, 3).t(3).cx(3, 4).measure(2, 2).h(2).reset(1).measure_all()
+    want = ref.run(qc, 300, 17, noise=noise)
+    got = counts_of(lq.StatevectorSimulator(seed=17, noise=noise, max_resident=resident)
+                    .run_registers(qc, 300))
+    assert got == want
+
+
+def test_explicit_kraus_placements_identical(ref):
+    qc = W.brickwork(6, 4, seed=3, measure=True, noise=(0.05, 0.1, 0.2))
+    want = counts_of(ref.trajectories(qc, 256, 21))
+    got = counts_of(lq.StatevectorSimulator(seed=21, max_resident=32).run_registers(qc, 256))
+    assert got == want
+
+
+def test_large_batch_trajectories_run():
+    qc = W.brickwork(16, 3, seed=4, measure=True, noise=(1e-3, 1e-2, 1e-3))
+    regs = lq.StatevectorSimulator(seed=5, max_resident=16).run_registers(qc, 40)
+    assert regs.shape == (40,)
+    regs2 = lq.StatevectorSimulator(seed=5, max_resident=40).run_registers(qc, 40)
+    assert np.array_equal(regs, regs2)
+
+
+def test_config3_cross_check_tvd(ref):
+    n, shots = 10, 1024
+    qc = W.brickwork(n, 20, seed=2026, measure=True, noise=(1e-3, 1e-2, 1e-3))
+    exact = ref.dm_probabilities(qc)
+    exact = exact / exact.sum()
+    regs = lq.StatevectorSimulator(seed=99, max_resident=256).run_registers(qc, shots)
+    freq = np.bincount(regs.astype(np.int64), minlength=1 << n) / shots
+    tvd = 0.5 * np.abs(freq - exact).sum()
+    rng = np.random.default_rng(12345)
+    boot = []
+    for _ in range(200):
+        draw = rng.choice(1 << n, size=shots, p=exact)
+        boot.append(0.5 * np.abs(np.bincount(draw, minlength=1 << n) / shots - exact).sum())
+    assert tvd <= np.quantile(boot, 0.999)
+    assert tvd >= np.quantile(boot, 0.001)
