@@ -432,6 +432,55 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     except Exception as ex:  # noqa: BLE001
         out["qft_error"] = str(ex)
 
+    # noisy trajectories: 26-qubit brickwork depth 20, depolarizing 1e-3 after each U3,
+    # 1e-2 on both qubits after each CX, amplitude damping 1e-3 per qubit per layer; one
+    # resident batch of 64 trajectories (a bounded sample of the 1024-trajectory run)
+    try:
+        tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+        sim = lq.StatevectorSimulator(seed=404, max_resident=64)
+        sim.run_registers(W.brickwork(10, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3)), 8)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.run_registers(tq, 64)
+        dt = time.perf_counter() - t0
+        out["trajectories_26q_per_s"] = 64 / dt
+        out["trajectories_26q_sample"] = "64 trajectories resident at once (1 GiB each), host-timed"
+    except Exception as ex:  # noqa: BLE001
+        out["trajectories_error"] = str(ex)
+
+    # learned fusion cost model: trained on the engine's own per-operation timings of
+    # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the
+    # greedy plan of a held-out 32-qubit circuit (64 GiB state) are timed on the device
+    try:
+        from litequantumcomputingsimulator_b200 import costmodel as CM
+        train_set = [W.random_mix_circuit(nq, d, s) for nq, d, s in
+                     [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14)]]
+        t0 = time.perf_counter()
+        x, y = CM.collect(train_set)
+        loss = CM.train(x, y, epochs=3000, lr=3e-3, seed=0)
+        out["costmodel_train_rows"] = int(y.size)
+        out["costmodel_train_mse"] = loss
+        out["costmodel_collect_train_s"] = time.perf_counter() - t0
+        held = W.random_mix_circuit(32, 16, seed=777)
+        big = lq.Statevector(32)
+        res = {}
+        for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED)):
+            prog = lq.simulator.CompiledCircuit(held, True, 0, mode)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            prog.apply(big)
+            e.record()
+            torch.cuda.synchronize()
+            res[name] = (s.elapsed_time(e), prog.n_ops)
+        out["costmodel_32q_greedy_ms"] = res["greedy"][0]
+        out["costmodel_32q_learned_ms"] = res["learned"][0]
+        out["costmodel_32q_ops"] = {"greedy": res["greedy"][1], "learned": res["learned"][1]}
+        out["costmodel_32q_speedup"] = res["greedy"][0] / res["learned"][0]
+        del big
+        torch.cuda.empty_cache()
+    except Exception as ex:  # noqa: BLE001
+        out["costmodel_error"] = str(ex)
+
     # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets)
     try:
         pc, _ = W.random_pauli_ansatz(16, 200, seed=11)

@@ -205,7 +205,7 @@ std::vector<FusedBlock> plan(const std::vector<GateDesc>& gates, uint32_t n,
 
 static bool use_tiles(uint32_t n, const FusionConfig& fc) {
     if (!fc.fuse) return false;
-    if (fc.mode == kFuseTile) return n >= 6;
+    if (fc.mode == kFuseTile) return n >= kTileMinBits;
     if (fc.mode == kFuseDefault) return n >= 12 && !std::getenv("LQCS_NO_TILES");
     return false;
 }
@@ -265,7 +265,7 @@ static Program compile_learned(const std::vector<GateDesc>& gates, uint32_t n,
             best_ops = std::move(ops);
         }
     }
-    if (n >= 6) {
+    if (n >= kTileMinBits) {
         const uint32_t shapes[][3] = {{11, 5, 2}, {12, 5, 2}, {12, 5, 3}, {13, 5, 2}, {13, 5, 3}};
         for (const auto& s : shapes) {
             TileConfig cfg;

@@ -9,25 +9,41 @@
 namespace lqcs_b200 {
 
 constexpr uint32_t kTileThreads = 256;
+constexpr uint32_t kTileMinBits = 8;             // a tile holds at least one amplitude per thread
 constexpr uint32_t kTileMaxBits = 13;            // 2^13 amplitudes = 128 KiB of shared memory
 constexpr uint32_t kTileMaxHigh = 8;             // at most 8 high qubits per tile
 constexpr uint32_t kTileMaxK = 4;                // widest dense operation inside a tile
-constexpr uint32_t kTileMaxOps = 512;            // operations per pass (staged in shared memory)
+constexpr uint32_t kTileMaxOps = 128;            // operations per pass (staged in shared memory)
+constexpr uint32_t kTileMaxIters = 32;           // 2^kTileMaxBits / kTileThreads
 constexpr size_t kTileMaxSmem = 200 * 1024;      // tile + staged operation records
 
 enum : uint8_t { kTileDense = 0, kTileDiag = 1, kTilePhase = 2 };
 
+// Shared-memory slot of tile element i: the low 3 bits are XOR-ed with a fold of the
+// higher bits so that power-of-two strides spread over the 8 16-byte positions of a
+// 128-byte wavefront.  The map is linear over GF(2): sw(a ^ b) == sw(a) ^ sw(b).
+__host__ __device__ __forceinline__ uint32_t tile_swizzle(uint32_t i) {
+    return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9) ^ (i >> 12)) & 7u);
+}
+
 // One operation on a tile, in tile-local bit positions (local bit j < L is qubit j, local
-// bit L + i is the i-th high qubit of the tile).
+// bit L + i is the i-th high qubit of the tile).  Groups (of 2^k amplitudes, or single
+// amplitudes of a phase) are numbered g = t + kTileThreads * j for thread t; because both
+// the zero-insertion that spreads g over the free bit positions and the swizzle are linear
+// over GF(2), the slot of member l of group g is
+//     sw(deposit(t)) ^ dhi[j] ^ soff[l],
+// with sw(deposit(t)) computed once per thread and operation and dhi, soff precomputed.
 struct TileOp {
     uint64_t gcmask;      // qubits outside the tile that must all be 1 (controls / phase bits)
-    uint32_t lcmask;      // dense/diag: local control bits; phase: local phase bits
     uint32_t mat_off;     // matrix (dense), diagonal (diag) or phase factor (phase), in double2
-    uint16_t loff[16];    // local offsets of the 2^k members of a group (matrix local order)
+    uint16_t n_groups;    // groups (dense, diag) or amplitudes (phase) to visit
+    uint16_t iters;       // ceil(n_groups / kTileThreads)
+    uint16_t soff[16];    // sw(local offset of member l), matrix local order
+    uint16_t dhi[kTileMaxIters];   // sw(deposit(j * kTileThreads) | local control bits)
     uint8_t kind;
     uint8_t k;
-    uint8_t n_fixed;      // number of local positions inserted as zeros when enumerating groups
-    uint8_t n_lctrl;      // popcount(lcmask) for dense/diag
+    uint8_t n_fixed;      // positions inserted as zeros when spreading a group index
+    uint8_t pad;
     uint8_t fixed[8];     // those positions, ascending
 };
 

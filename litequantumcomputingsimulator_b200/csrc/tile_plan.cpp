@@ -36,8 +36,8 @@ TileConfig default_tile_config(uint32_t n) {
     c.m = static_cast<uint32_t>(env_int("LQCS_TILE_BITS", 12));
     c.L = static_cast<uint32_t>(env_int("LQCS_TILE_LOW", 5));
     c.inner = static_cast<uint32_t>(env_int("LQCS_TILE_INNER", 2));
-    c.m = std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n);
-    c.L = std::min(c.L, c.m);
+    c.m = std::max<uint32_t>(kTileMinBits, std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n));
+    c.L = std::min<uint32_t>(std::min(c.L, c.m), kTileMinBits);   // column bits come from the thread index
     if (c.m - c.L > kTileMaxHigh) c.L = c.m - kTileMaxHigh;
     c.inner = std::max<uint32_t>(1, std::min<uint32_t>(c.inner, kTileMaxK));
     return c;
@@ -116,6 +116,9 @@ std::vector<PlanItem> plan_tiles(const std::vector<GateDesc>& gates, uint32_t n,
             remaining.erase(remaining.begin());
             continue;
         }
+        // every pass gets the full tile size: pad H with unused high qubits
+        for (uint32_t q = cfg.L; q < n && hset.size() < h; ++q)
+            if (std::find(hset.begin(), hset.end(), q) == hset.end()) hset.push_back(q);
         PlanItem it;
         it.is_pass = true;
         std::sort(hset.begin(), hset.end());
@@ -141,15 +144,30 @@ struct LocalMap {
     }
 };
 
-void set_fixed(TileOp& op, std::vector<uint32_t> pos) {
+uint32_t deposit(uint32_t v, const std::vector<uint32_t>& sorted_pos) {
+    for (uint32_t p : sorted_pos) {
+        const uint32_t low = (1u << p) - 1u;
+        v = ((v & ~low) << 1) | (v & low);
+    }
+    return v;
+}
+
+// Group enumeration of an op on a 2^m tile: the positions spread over (ascending), the
+// group count, and the per-iteration slot parts sw(deposit(j * threads) | lcmask).
+void set_groups(TileOp& op, std::vector<uint32_t> pos, uint32_t lcmask, uint32_t m) {
     std::sort(pos.begin(), pos.end());
     op.n_fixed = static_cast<uint8_t>(pos.size());
     for (size_t i = 0; i < pos.size(); ++i) op.fixed[i] = static_cast<uint8_t>(pos[i]);
+    const uint32_t groups = (1u << m) >> pos.size();
+    op.n_groups = static_cast<uint16_t>(groups);
+    op.iters = static_cast<uint16_t>(std::max<uint32_t>(1, groups / kTileThreads));
+    for (uint32_t j = 0; j < op.iters; ++j)
+        op.dhi[j] = static_cast<uint16_t>(tile_swizzle(deposit(j * kTileThreads, pos) | lcmask));
 }
 
 // Dense or diagonal op of matrix m on local target positions lt (matrix local order).
 TileOp make_matrix_op(const std::vector<cd>& m, const std::vector<uint32_t>& lt, uint32_t lcmask,
-                      uint64_t gcmask, std::vector<cd>& arena) {
+                      uint64_t gcmask, std::vector<cd>& arena, uint32_t tile_bits) {
     TileOp op{};
     const uint32_t k = static_cast<uint32_t>(lt.size());
     const uint64_t dim = uint64_t{1} << k;
@@ -159,19 +177,17 @@ TileOp make_matrix_op(const std::vector<cd>& m, const std::vector<uint32_t>& lt,
             if (r != c && m[r * dim + c] != cd{0, 0}) { diag = false; break; }
     op.kind = diag ? kTileDiag : kTileDense;
     op.k = static_cast<uint8_t>(k);
-    op.lcmask = lcmask;
     op.gcmask = gcmask;
-    op.n_lctrl = static_cast<uint8_t>(__builtin_popcount(lcmask));
     for (uint64_t l = 0; l < dim; ++l) {
         uint32_t o = 0;
         for (uint32_t j = 0; j < k; ++j)
             if ((l >> j) & 1) o |= 1u << lt[j];
-        op.loff[l] = static_cast<uint16_t>(o);
+        op.soff[l] = static_cast<uint16_t>(tile_swizzle(o));
     }
     std::vector<uint32_t> fixed = lt;
     for (uint32_t b = 0; b < 32; ++b)
         if ((lcmask >> b) & 1) fixed.push_back(b);
-    set_fixed(op, fixed);
+    set_groups(op, fixed, lcmask, tile_bits);
     op.mat_off = static_cast<uint32_t>(arena.size());
     if (diag) {
         for (uint64_t i = 0; i < dim; ++i) arena.push_back(m[i * dim + i]);
@@ -212,23 +228,24 @@ void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const 
         fb.qubits = b.qubits;
         fb.gates = b.gates;
         const std::vector<cd> m = block_matrix(fb, gates);
-        ops_out.push_back(make_matrix_op(m, lt, 0, 0, arena));
+        ops_out.push_back(make_matrix_op(m, lt, 0, 0, arena, pass.m));
     };
     auto emit_single = [&](const GateDesc& g) {
         if (is_phase_gate(g)) {
             TileOp op{};
             op.kind = kTilePhase;
             std::vector<uint32_t> fixed;
+            uint32_t lmask = 0;
             for (uint32_t q : g.qubits) {
                 const int l = lm.local(q);
                 if (l >= 0) {
-                    op.lcmask |= 1u << l;
+                    lmask |= 1u << l;
                     fixed.push_back(static_cast<uint32_t>(l));
                 } else {
                     op.gcmask |= uint64_t{1} << q;
                 }
             }
-            set_fixed(op, fixed);
+            set_groups(op, fixed, lmask, pass.m);
             op.mat_off = static_cast<uint32_t>(arena.size());
             arena.push_back(g.base_matrix()[3]);
             ops_out.push_back(op);
@@ -245,7 +262,7 @@ void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const 
             if (l >= 0) lc |= 1u << l;
             else gc |= uint64_t{1} << q;
         }
-        ops_out.push_back(make_matrix_op(g.base_matrix(), lt, lc, gc, arena));
+        ops_out.push_back(make_matrix_op(g.base_matrix(), lt, lc, gc, arena, pass.m));
     };
 
     for (uint32_t gi : item.gates) {
