@@ -185,7 +185,8 @@ int lqcs_program_apply(lqcs_state* st, const lqcs_program* prog);
  * state's stream. */
 typedef struct lqcs_op_profile {
     uint32_t kind;          /* 0 one-qubit, 1 phase, 2 dense block, 3 diagonal block,
-                               4 permutation, 5 Pauli rotation */
+                               4 permutation, 5 Pauli rotation, 6 shared-memory tile pass,
+                               7 register tile pass */
     uint32_t n_targets;     /* block width */
     uint32_t n_gates;       /* source gates merged into the operation */
     uint32_t min_target;
@@ -351,7 +352,7 @@ int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t 
  * counterpart in the reference.  Targets are log(milliseconds per 2^24 amplitudes). */
 enum { LQCS_COST_FEATURES = 6, LQCS_COST_HIDDEN = 64 };
 
-/* Feature row of one operation (kind as in lqcs_op_profile, or 6 for a tile pass). */
+/* Feature row of one operation (kind as in lqcs_op_profile). */
 int lqcs_costmodel_features(uint32_t kind, uint32_t width, uint32_t min_target,
                             uint32_t max_target, uint32_t n_gates, uint32_t n_qubits,
                             float* out);

@@ -98,7 +98,7 @@ class OpProfile(C.Structure):
 
 
 OP_KIND_NAMES = {0: "k_apply_1q", 1: "k_phase", 2: "k_dense", 3: "k_diag", 4: "k_perm",
-                 5: "k_pauli", 6: "k_tile"}
+                 5: "k_pauli", 6: "k_tile", 7: "k_regtile"}
 
 StatePtr = C.c_void_p
 ProgramPtr = C.c_void_p

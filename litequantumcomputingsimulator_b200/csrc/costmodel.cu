@@ -328,7 +328,7 @@ std::array<float, kCostFeatures> op_features(const DevOp& op, uint32_t n) {
     for (uint32_t t : op.targets) mask |= uint64_t{1} << t;
     const uint32_t lo = mask ? static_cast<uint32_t>(__builtin_ctzll(mask)) : 0;
     const uint32_t hi = mask ? 63u - static_cast<uint32_t>(__builtin_clzll(mask)) : 0;
-    return op_features(static_cast<uint32_t>(op.kind), op.k, lo, hi, op.src_gates, n);
+    return op_features(profile_kind(op), op.k, lo, hi, op.src_gates, n);
 }
 
 double predict_ops_ms(const std::vector<DevOp>& ops, uint32_t n) {

@@ -122,6 +122,25 @@ void Program::build(std::vector<DevOp> ops_in, cudaStream_t stream) {
                                    cudaMemcpyHostToDevice, stream),
                    "upload tile matrices");
     }
+    std::vector<double2> rmats;
+    for (const cd& z : reg_mats) rmats.push_back(to_d2(z));
+    if (!reg_ops.empty()) {
+        d_reg_ops.ensure(reg_ops.size() * sizeof(RegOp));
+        cuda_check(cudaMemcpyAsync(d_reg_ops.ptr, reg_ops.data(), reg_ops.size() * sizeof(RegOp),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload register pass records");
+        d_reg_layouts.ensure(reg_layouts.size() * sizeof(RegLayout));
+        cuda_check(cudaMemcpyAsync(d_reg_layouts.ptr, reg_layouts.data(),
+                                   reg_layouts.size() * sizeof(RegLayout), cudaMemcpyHostToDevice,
+                                   stream),
+                   "upload register layouts");
+    }
+    if (!rmats.empty()) {
+        d_reg_mats.ensure(rmats.size() * sizeof(double2));
+        cuda_check(cudaMemcpyAsync(d_reg_mats.ptr, rmats.data(), rmats.size() * sizeof(double2),
+                                   cudaMemcpyHostToDevice, stream),
+                   "upload register pass matrices");
+    }
     // the host vectors die with this scope: make sure the copies have consumed them
     cuda_check(cudaStreamSynchronize(stream), "program upload");
 }
@@ -162,6 +181,13 @@ void Program::launch_op(size_t i, const LaunchCtx& ctx, double2* st, uint32_t n,
             launch_pauli_rotation(ctx, st, n, batch, op.x, op.zy, op.n_y, op.cos_h, op.sin_h);
             break;
         case OpKind::TILE:
+            if (op.reg_tile) {
+                launch_reg_pass(ctx, st, n, batch, reg_passes[op.pass_index],
+                                d_reg_ops.as<RegOp>() + reg_op_off[op.pass_index],
+                                d_reg_layouts.as<RegLayout>() + reg_lay_off[op.pass_index],
+                                d_reg_mats.as<double2>() + reg_mat_off[op.pass_index]);
+                break;
+            }
             launch_tile_pass(ctx, st, n, batch, passes[op.pass_index],
                              d_tile_ops.as<TileOp>() + pass_op_off[op.pass_index],
                              d_tile_mats.as<double2>());
@@ -219,16 +245,30 @@ static Program assemble_tiles(const std::vector<GateDesc>& gates, uint32_t n,
             ops.push_back(lower_gate(gates[it.gate], n));
             continue;
         }
+        DevOp op;
+        op.kind = OpKind::TILE;
+        op.k = static_cast<uint32_t>(it.hbits.size());
+        op.targets = it.hbits;
+        op.src_gates = static_cast<uint32_t>(it.gates.size());
+        op.alg_fraction = 1.0;
+        if (cfg.reg) {
+            RegPass rp;
+            const size_t o0 = p.reg_ops.size(), l0 = p.reg_layouts.size(), m0 = p.reg_mats.size();
+            if (lower_pass_reg(it, gates, cfg, rp, p.reg_ops, p.reg_layouts, p.reg_mats)) {
+                p.reg_op_off.push_back(o0);
+                p.reg_lay_off.push_back(l0);
+                p.reg_mat_off.push_back(m0);
+                op.reg_tile = true;
+                op.pass_index = static_cast<uint32_t>(p.reg_passes.size());
+                p.reg_passes.push_back(rp);
+                ops.push_back(std::move(op));
+                continue;
+            }
+        }
         TilePass tp;
         p.pass_op_off.push_back(p.tile_ops.size());
         lower_pass(it, gates, cfg, tp, p.tile_ops, p.tile_mats);
-        DevOp op;
-        op.kind = OpKind::TILE;
-        op.k = tp.h;
-        op.targets = it.hbits;
         op.pass_index = static_cast<uint32_t>(p.passes.size());
-        op.src_gates = static_cast<uint32_t>(it.gates.size());
-        op.alg_fraction = 1.0;
         p.passes.push_back(tp);
         ops.push_back(std::move(op));
     }
@@ -412,7 +452,7 @@ void program_profile(lqcs_state& st, const lqcs_program& p, uint64_t cap, lqcs_o
         float ms = 0.0f;
         cuda_check(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "cudaEventElapsedTime");
         lqcs_op_profile& r = out[i];
-        r.kind = static_cast<uint32_t>(op.kind);
+        r.kind = profile_kind(op);
         r.n_targets = op.k;
         r.n_gates = op.src_gates;
         r.min_target = op.targets.empty() ? 0 : *std::min_element(op.targets.begin(), op.targets.end());

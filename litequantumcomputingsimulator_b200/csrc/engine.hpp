@@ -57,6 +57,13 @@ struct Program {
     std::vector<TileOp> tile_ops;
     std::vector<cd> tile_mats;
     DeviceBuffer d_tile_ops, d_tile_mats;
+    // register tile passes (ops of kind TILE with reg_tile set index into these)
+    std::vector<RegPass> reg_passes;
+    std::vector<uint64_t> reg_op_off, reg_lay_off, reg_mat_off;   // per pass
+    std::vector<RegOp> reg_ops;
+    std::vector<RegLayout> reg_layouts;
+    std::vector<cd> reg_mats;
+    DeviceBuffer d_reg_ops, d_reg_layouts, d_reg_mats;
 
     void build(std::vector<DevOp> ops_in, cudaStream_t stream);
     void launch(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch) const;

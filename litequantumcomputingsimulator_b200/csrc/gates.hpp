@@ -87,12 +87,19 @@ struct DevOp {
     uint64_t x = 0, zy = 0;
     uint32_t n_y = 0;
     double cos_h = 1.0, sin_h = 0.0;
-    // TILE: index of the shared-memory pass in the program
+    // TILE: index of the pass in the program's shared-memory or register pass list
     uint32_t pass_index = 0;
+    bool reg_tile = false;
     // bookkeeping
     uint32_t src_gates = 1;              // source gates merged into this op
     double alg_fraction = 1.0;           // fraction of amplitudes it can change
 };
+
+// Kind number of an op in profiles and cost-model features: the OpKind, or 7 for a tile
+// pass run by the register kernel.
+inline uint32_t profile_kind(const DevOp& op) {
+    return op.kind == OpKind::TILE && op.reg_tile ? 7u : static_cast<uint32_t>(op.kind);
+}
 
 // Lower one unitary gate to a device op following the dispatch of apply_instruction
 // (src/backend/statevector_simulator.cpp:22-85) — plus a PHASE fast path for diagonal

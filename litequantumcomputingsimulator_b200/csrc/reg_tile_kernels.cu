@@ -1,0 +1,445 @@
+// reg_tile_kernels.cu — multi-gate passes with the tile held in registers.
+//
+// Same passes as tile_kernels.cu (one HBM read and write of the state applies a whole list
+// of operations), with a different home for the tile: each thread keeps 16 amplitudes in
+// registers and shared memory only serves the remaps that change which 4 tile bits are
+// register bits (see RegLayout).  Per amplitude and operation the shared-memory kernel
+// moves 32 bytes through shared memory; here a dense operation on register bits moves
+// none, so the pass runs at the FP64 rate instead of the shared-memory rate.
+//
+// Operation semantics follow the reference kernels (src/backend/kernels/gate_kernels.cpp):
+// a dense operation is a 2^k x 2^k matrix on its targets applied where every control is 1;
+// a diagonal operation multiplies by the entry its target bits select; a phase operation
+// multiplies the amplitudes whose phase bits are all 1.
+#include <algorithm>
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+
+#include "kernels.cuh"
+#include "tile.cuh"
+
+namespace lqcs_b200 {
+
+namespace {
+
+constexpr int kE = 1 << kRegBits;   // amplitudes per thread
+
+void check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string("CUDA launch failed in ") + what + ": " +
+                                 cudaGetErrorString(e));
+    }
+    count_launch();
+}
+
+__host__ __device__ constexpr int popc4(int m) {
+    return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1);
+}
+
+// Member l of a group: the bits of l spread over the set bits of mask, lowest first.
+__host__ __device__ constexpr int deposit4(int l, int mask) {
+    int out = 0, j = 0;
+    for (int b = 0; b < kRegBits; ++b) {
+        if ((mask >> b) & 1) {
+            if ((l >> j) & 1) out |= 1 << b;
+            ++j;
+        }
+    }
+    return out;
+}
+
+// Shared-memory load the compiler may not hoist or merge: matrix entries are re-read per
+// group so they never occupy registers alongside the 16 amplitudes.
+__device__ __forceinline__ double2 lds2(uint32_t saddr) {
+    double2 r;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "r"(saddr));
+    return r;
+}
+
+// Group base of the g-th group of a target mask: g spread over the bits outside TM.
+__host__ __device__ constexpr int group_base(int g, int tm) { return deposit4(g, (kE - 1) & ~tm); }
+
+// Dense operation without register controls: one basic block, so the compiler interleaves
+// the groups.  Two-target operations take two groups per matrix read (each entry is loaded
+// twice per operation instead of four times).
+template <int TM>
+__device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
+    constexpr int K = popc4(TM);
+    constexpr int D = 1 << K;
+    constexpr int G = kE / D;   // groups
+    if constexpr (K == 1) {
+        const double2 m0 = lds2(mat), m1 = lds2(mat + 16), m2 = lds2(mat + 32), m3 = lds2(mat + 48);
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int b = group_base(g, TM);
+            const double2 a0 = v[b], a1 = v[b | TM];
+            v[b] = cmad(m1, a1, cmul(m0, a0));
+            v[b | TM] = cmad(m3, a1, cmul(m2, a0));
+        }
+    } else if constexpr (K == 2) {
+#pragma unroll
+        for (int g = 0; g < G; g += 2) {
+            const int b0 = group_base(g, TM), b1 = group_base(g + 1, TM);
+            double2 y0[D], y1[D];
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                const double2 mr = lds2(mat + 16u * (r * D));
+                y0[r] = cmul(mr, v[b0]);
+                y1[r] = cmul(mr, v[b1]);
+            }
+#pragma unroll
+            for (int c = 1; c < D; ++c) {
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    const double2 mr = lds2(mat + 16u * (r * D + c));
+                    y0[r] = cmad(mr, v[b0 | deposit4(c, TM)], y0[r]);
+                    y1[r] = cmad(mr, v[b1 | deposit4(c, TM)], y1[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                v[b0 | deposit4(r, TM)] = y0[r];
+                v[b1 | deposit4(r, TM)] = y1[r];
+            }
+        }
+    } else {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int b = group_base(g, TM);
+            double2 y[D];
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                double2 acc = cmul(lds2(mat + 16u * (r * D)), v[b]);
+#pragma unroll
+                for (int c = 1; c < D; ++c)
+                    acc = cmad(lds2(mat + 16u * (r * D + c)), v[b | deposit4(c, TM)], acc);
+                y[r] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < D; ++r) v[b | deposit4(r, TM)] = y[r];
+        }
+    }
+}
+
+// Dense operation with register controls: groups whose control bits are not all 1 skip.
+template <int TM>
+__device__ __forceinline__ void reg_dense(double2 (&v)[kE], uint32_t mat, uint32_t rcmask) {
+    constexpr int K = popc4(TM);
+    constexpr int D = 1 << K;
+    if constexpr (K == 1) {
+        const double2 m0 = lds2(mat), m1 = lds2(mat + 16), m2 = lds2(mat + 32), m3 = lds2(mat + 48);
+#pragma unroll
+        for (int b = 0; b < kE; ++b) {
+            if (b & TM) continue;
+            if ((b & rcmask) != rcmask) continue;
+            const double2 a0 = v[b], a1 = v[b | TM];
+            v[b] = cmad(m1, a1, cmul(m0, a0));
+            v[b | TM] = cmad(m3, a1, cmul(m2, a0));
+        }
+    } else {
+#pragma unroll
+        for (int b = 0; b < kE; ++b) {
+            if (b & TM) continue;
+            if ((b & rcmask) != rcmask) continue;
+            double2 y[D];
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                double2 acc = cmul(lds2(mat + 16u * (r * D)), v[b | deposit4(0, TM)]);
+#pragma unroll
+                for (int c = 1; c < D; ++c)
+                    acc = cmad(lds2(mat + 16u * (r * D + c)), v[b | deposit4(c, TM)], acc);
+                y[r] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < D; ++r) v[b | deposit4(r, TM)] = y[r];
+        }
+    }
+}
+
+template <int I>
+__device__ __forceinline__ void reg_swapx(double2 (&v)[kE], uint32_t rcmask) {
+#pragma unroll
+    for (int b = 0; b < kE; ++b) {
+        if ((b >> I) & 1) continue;
+        if ((b & rcmask) != rcmask) continue;
+        const double2 a = v[b];
+        v[b] = v[b | (1 << I)];
+        v[b | (1 << I)] = a;
+    }
+}
+
+__device__ __forceinline__ void dispatch_dense(double2 (&v)[kE], uint32_t code, uint32_t mat,
+                                               uint32_t rcmask) {
+    if (rcmask == 0) {
+        switch (code) {
+            case 1: reg_dense_free<1>(v, mat); break;
+            case 2: reg_dense_free<2>(v, mat); break;
+            case 3: reg_dense_free<3>(v, mat); break;
+            case 4: reg_dense_free<4>(v, mat); break;
+            case 5: reg_dense_free<5>(v, mat); break;
+            case 6: reg_dense_free<6>(v, mat); break;
+            case 7: reg_dense_free<7>(v, mat); break;
+            case 8: reg_dense_free<8>(v, mat); break;
+            case 9: reg_dense_free<9>(v, mat); break;
+            case 10: reg_dense_free<10>(v, mat); break;
+            case 11: reg_dense_free<11>(v, mat); break;
+            case 12: reg_dense_free<12>(v, mat); break;
+            case 13: reg_dense_free<13>(v, mat); break;
+            case 14: reg_dense_free<14>(v, mat); break;
+            default: break;
+        }
+        return;
+    }
+    switch (code) {
+        case 1: reg_dense<1>(v, mat, rcmask); break;
+        case 2: reg_dense<2>(v, mat, rcmask); break;
+        case 3: reg_dense<3>(v, mat, rcmask); break;
+        case 4: reg_dense<4>(v, mat, rcmask); break;
+        case 5: reg_dense<5>(v, mat, rcmask); break;
+        case 6: reg_dense<6>(v, mat, rcmask); break;
+        case 7: reg_dense<7>(v, mat, rcmask); break;
+        case 8: reg_dense<8>(v, mat, rcmask); break;
+        case 9: reg_dense<9>(v, mat, rcmask); break;
+        case 10: reg_dense<10>(v, mat, rcmask); break;
+        case 11: reg_dense<11>(v, mat, rcmask); break;
+        case 12: reg_dense<12>(v, mat, rcmask); break;
+        case 13: reg_dense<13>(v, mat, rcmask); break;
+        case 14: reg_dense<14>(v, mat, rcmask); break;
+        default: break;   // 4-target operations never reach a register pass
+    }
+}
+
+__device__ __forceinline__ void dispatch_swapx(double2 (&v)[kE], uint32_t code, uint32_t rcmask) {
+    switch (code) {
+        case 1: reg_swapx<0>(v, rcmask); break;
+        case 2: reg_swapx<1>(v, rcmask); break;
+        case 4: reg_swapx<2>(v, rcmask); break;
+        default: reg_swapx<3>(v, rcmask); break;
+    }
+}
+
+// Entry (tpart | bits picked from u) of a diagonal for every amplitude u.
+__device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, uint32_t mat,
+                                         uint32_t rcmask) {
+    uint32_t tpart = 0, rb0 = 0, rb1 = 0, rb2 = 0, rb3 = 0;   // entry bit of register bit i
+    const uint32_t k = op.k;
+    for (uint32_t j = 0; j < k; ++j) {
+        const uint32_t loc = op.loc[j], bit = 1u << j;
+        if (loc & 0x80u) {
+            tpart |= ((threadIdx.x >> (loc & 0x7fu)) & 1u) << j;
+        } else {
+            rb0 |= loc == 0 ? bit : 0u;
+            rb1 |= loc == 1 ? bit : 0u;
+            rb2 |= loc == 2 ? bit : 0u;
+            rb3 |= loc == 3 ? bit : 0u;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kE; ++u) {
+        if ((u & rcmask) != rcmask) continue;
+        const uint32_t e = tpart | ((u & 1) ? rb0 : 0u) | ((u & 2) ? rb1 : 0u) |
+                           ((u & 4) ? rb2 : 0u) | ((u & 8) ? rb3 : 0u);
+        v[u] = cmul(lds2(mat + 16u * e), v[u]);
+    }
+}
+
+__device__ __forceinline__ uint32_t thread_slot(const RegLayout& ly, uint32_t tbits) {
+    uint32_t s = 0;
+    for (uint32_t i = 0; i < tbits; ++i)
+        if ((threadIdx.x >> i) & 1u) s ^= ly.tsw[i];
+    return s;
+}
+
+__device__ __forceinline__ uint64_t thread_goff(const RegLayout& ly, uint32_t tbits,
+                                                const uint64_t* gbit) {
+    uint64_t g = 0;
+    for (uint32_t i = 0; i < tbits; ++i)
+        if ((threadIdx.x >> i) & 1u) g |= gbit[ly.tpos[i]];
+    return g;
+}
+
+// MINB resident CTAs per SM: registers per thread <= 65536 / (MINB * threads).
+template <int M, int MINB>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
+k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
+          const RegLayout* __restrict__ layouts, const double2* __restrict__ mats) {
+    constexpr uint32_t kT = 1u << (M - kRegBits);
+    constexpr uint32_t kTB = M - kRegBits;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* __restrict__ tile = reinterpret_cast<double2*>(smem);
+    double2* smat = tile + (1u << M);
+    RegOp* sops = reinterpret_cast<RegOp*>(smat + p.n_mat);
+    RegLayout* slay = reinterpret_cast<RegLayout*>(sops + p.n_ops);
+    __shared__ uint64_t gbit[kRegMaxBits];   // global offset of each tile bit
+    __shared__ uint32_t shbits[kTileMaxHigh];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (uint32_t i = 0; i < kTileMaxHigh; ++i) shbits[i] = p.hbits[i];   // static indices
+        for (uint32_t b = 0; b < M; ++b)
+            gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
+    }
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(mats);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(smat);
+        for (uint32_t w = threadIdx.x; w < p.n_mat * 4u; w += kT) dst[w] = src[w];
+        src = reinterpret_cast<const uint32_t*>(ops);
+        dst = reinterpret_cast<uint32_t*>(sops);
+        for (uint32_t w = threadIdx.x; w < p.n_ops * (sizeof(RegOp) / 4); w += kT) dst[w] = src[w];
+        src = reinterpret_cast<const uint32_t*>(layouts);
+        dst = reinterpret_cast<uint32_t*>(slay);
+        for (uint32_t w = threadIdx.x; w < p.n_layouts * (sizeof(RegLayout) / 4); w += kT)
+            dst[w] = src[w];
+    }
+    __syncthreads();
+    const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
+    double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
+    for (uint64_t tid = blockIdx.x; tid < p.n_tiles; tid += gridDim.x) {
+        uint64_t base = tid << p.L;
+        for (uint32_t i = 0; i < p.h; ++i) base = insert_zero_bit(base, shbits[i]);
+        double2 v[kE];
+        {
+            const RegLayout& ly = slay[0];
+            const uint64_t g = base | thread_goff(ly, kTB, gbit);
+            const uint64_t g0 = gbit[ly.rpos[0]], g1 = gbit[ly.rpos[1]], g2 = gbit[ly.rpos[2]],
+                           g3 = gbit[ly.rpos[3]];
+#pragma unroll
+            for (int u = 0; u < kE; ++u)
+                v[u] = __ldcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
+                                   ((u & 8) ? g3 : 0)));
+        }
+        uint32_t cur = 0;
+        for (uint32_t o = 0; o < p.n_ops; ++o) {
+            const RegOp& op = sops[o];
+            if ((base & op.gcmask) != op.gcmask) continue;   // uniform across the CTA
+            const uint32_t kind = op.kind;
+            if (kind == kRegRemap) {
+                {
+                    const RegLayout& ly = slay[cur];
+                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
+#pragma unroll
+                    for (int u = 0; u < kE; ++u)
+                        tile[ts ^ ((u & 1) ? r0 : 0) ^ ((u & 2) ? r1 : 0) ^ ((u & 4) ? r2 : 0) ^
+                             ((u & 8) ? r3 : 0)] = v[u];
+                }
+                cur = op.code;
+                __syncthreads();
+                {
+                    const RegLayout& ly = slay[cur];
+                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
+#pragma unroll
+                    for (int u = 0; u < kE; ++u)
+                        v[u] = tile[ts ^ ((u & 1) ? r0 : 0) ^ ((u & 2) ? r1 : 0) ^
+                                    ((u & 4) ? r2 : 0) ^ ((u & 8) ? r3 : 0)];
+                }
+                __syncthreads();
+                continue;
+            }
+            const uint32_t tc = op.tcmask;
+            if ((threadIdx.x & tc) != tc) continue;
+            const uint32_t rc = op.rcmask;
+            uint32_t moff = op.mat_off;
+            if (const uint32_t nsel = op.nsel) {   // matrix picked by the tile's selector bits
+                uint32_t sel = 0;
+                for (uint32_t i = 0; i < nsel; ++i)
+                    sel |= static_cast<uint32_t>((base >> op.selq[i]) & 1u) << i;
+                const uint32_t k2 = kind == kRegDense ? 2u * op.k : op.k;
+                moff += sel << k2;
+            }
+            const uint32_t mat = smat_addr + 16u * moff;
+            if (kind == kRegDense) {
+                dispatch_dense(v, op.code, mat, rc);
+            } else if (kind == kRegPhase) {
+                const double2 f = lds2(mat);
+#pragma unroll
+                for (int u = 0; u < kE; ++u)
+                    if ((u & rc) == rc) v[u] = cmul(f, v[u]);
+            } else if (kind == kRegSwapX) {
+                dispatch_swapx(v, op.code, rc);
+            } else {
+                reg_diag(v, op, mat, rc);
+            }
+        }
+        {
+            const RegLayout& ly = slay[cur];
+            const uint64_t g = base | thread_goff(ly, kTB, gbit);
+            const uint64_t g0 = gbit[ly.rpos[0]], g1 = gbit[ly.rpos[1]], g2 = gbit[ly.rpos[2]],
+                           g3 = gbit[ly.rpos[3]];
+#pragma unroll
+            for (int u = 0; u < kE; ++u)
+                __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
+                            ((u & 8) ? g3 : 0)),
+                       v[u]);
+        }
+    }
+}
+
+template <int M, int MINB>
+void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
+               const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
+    constexpr uint32_t kT = 1u << (M - kRegBits);
+    auto kern = k_regtile<M, MINB>;
+    cuda_check_launch_attr(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(kTileMaxSmem)));
+    const uint32_t by_smem = static_cast<uint32_t>(std::max<size_t>(1, (227 * 1024) / (smem + 1024)));
+    const uint64_t want = static_cast<uint64_t>(ctx.num_sms) * std::min<uint32_t>(MINB, by_smem);
+    const uint32_t grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, p.n_tiles)));
+    kern<<<dim3(grid, batch), kT, smem, ctx.stream>>>(st, p, d_ops, d_layouts, d_mats);
+    check_launch("register tile pass");
+}
+
+// Residency per tile size: about 160 registers per thread keep the dense paths free of
+// spills, so M <= 11 run 168-register CTAs (12 warps per SM).  M = 12 runs two CTAs of 128
+// registers (a few spilled values; measured faster than one 160-register CTA, which
+// LQCS_TILE_OCC=1 selects); M = 13 (512 threads) is capped at 128.
+template <int M>
+void launch_m(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
+              const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
+    if constexpr (M == 12) {
+        static const int occ = [] {
+            const char* e = std::getenv("LQCS_TILE_OCC");
+            return e ? std::atoi(e) : 2;
+        }();
+        if (occ >= 2) {
+            launch_mb<12, 2>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+            return;
+        }
+        launch_mb<12, 1>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    } else if constexpr (M == 13) {
+        launch_mb<13, 1>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    } else {
+        constexpr int kMinB = 65536 / ((1 << (M - kRegBits)) * 168);
+        launch_mb<M, kMinB>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    }
+}
+
+}  // namespace
+
+size_t reg_smem_bytes(const RegPass& pass) {
+    return sizeof(double2) * ((size_t{1} << pass.m) + pass.n_mat) + sizeof(RegOp) * pass.n_ops +
+           sizeof(RegLayout) * pass.n_layouts;
+}
+
+void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
+                     const RegPass& pass, const RegOp* d_ops, const RegLayout* d_layouts,
+                     const double2* d_mats) {
+    RegPass p = pass;
+    p.batch_stride = uint64_t{1} << n;
+    p.n_tiles = (uint64_t{1} << n) >> p.m;
+    const size_t smem = reg_smem_bytes(p);
+    if (smem > kTileMaxSmem || p.m < kRegMinBits || p.m > kRegMaxBits || p.h > kTileMaxHigh ||
+        p.n_layouts < 1 || p.n_ops > kRegMaxRecords || p.n_mat > kRegMaxMatrix)
+        throw std::logic_error("register tile pass: unsupported shape");
+    switch (p.m) {
+        case 9: launch_m<9>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;
+        case 10: launch_m<10>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;
+        case 11: launch_m<11>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;
+        case 12: launch_m<12>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;
+        default: launch_m<13>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;
+    }
+}
+
+}  // namespace lqcs_b200

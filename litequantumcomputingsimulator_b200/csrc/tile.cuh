@@ -65,4 +65,63 @@ void launch_tile_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t ba
 size_t tile_smem_bytes(const TilePass& pass);
 void cuda_check_launch_attr(cudaError_t e);
 
+// ------------------------------------------------------------------ register tile passes
+//
+// The same passes with the tile held in registers: each of the 2^(m-4) threads of a CTA
+// owns 16 amplitudes.  A layout assigns 4 tile bits to the register index (amplitude u of
+// a thread has bit i of u at tile bit rpos[i]) and the other m-4 tile bits to the thread
+// index.  Dense operations whose targets are register bits run without shared memory;
+// diagonal and phase operations run in any layout; a remap operation moves the tile to the
+// next layout through shared memory.  Every remap, tile load and tile store is one pass of
+// the tile through shared memory or HBM, so a pass costs (remaps + 2) tile transfers
+// instead of (operations + 2).
+constexpr uint32_t kRegBits = 4;                // amplitudes per thread: 16
+constexpr uint32_t kRegMinBits = 9;             // a tile spans at least one warp
+constexpr uint32_t kRegMaxBits = 13;
+constexpr uint32_t kRegMaxK = 3;                // widest dense operation
+constexpr uint32_t kRegMaxRecords = 256;        // operations + remaps per pass
+constexpr uint32_t kRegMaxLayouts = 128;
+constexpr uint32_t kRegMaxMatrix = 2048;        // double2 of matrices staged per pass (32 KiB)
+constexpr uint32_t kRegMaxSelect = 2;           // out-of-tile selector qubits per operation
+
+enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4 };
+
+struct RegLayout {
+    uint16_t rsw[kRegBits];   // tile_swizzle(1 << rpos[i])
+    uint16_t tsw[9];          // tile_swizzle(1 << tpos[i])
+    uint8_t rpos[kRegBits];   // tile bit of register-index bit i
+    uint8_t tpos[9];          // tile bit of thread-index bit i
+    uint8_t pad[1];
+};
+
+struct RegOp {
+    uint64_t gcmask;          // qubits outside the tile that must all be 1
+    uint32_t mat_off;         // double2 offset in the pass's staged matrices
+    uint8_t kind;
+    uint8_t code;             // dense / swap: register target mask; remap: new layout index
+    uint8_t k;                // dense / diag: number of targets
+    uint8_t rcmask;           // register-index bits that must be 1 (controls, phase bits)
+    uint16_t tcmask;          // thread-index bits that must be 1
+    uint8_t loc[4];           // diag: target j at register bit loc, or thread bit loc & 0x7f
+                              // when loc & 0x80
+    uint8_t nsel;             // dense / diag: the tile's bits at qubits selq[0..nsel) pick
+    uint8_t selq[kRegMaxSelect];   // one of 2^nsel consecutive matrices
+    uint8_t pad[7];
+};
+
+struct RegPass {
+    uint64_t n_tiles;
+    uint64_t batch_stride;
+    uint32_t m, L, h;
+    uint32_t n_ops, n_layouts, n_mat;
+    uint32_t hbits[kTileMaxHigh];
+};
+
+static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");
+
+void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
+                     const RegPass& pass, const RegOp* d_ops, const RegLayout* d_layouts,
+                     const double2* d_mats);
+size_t reg_smem_bytes(const RegPass& pass);
+
 }  // namespace lqcs_b200

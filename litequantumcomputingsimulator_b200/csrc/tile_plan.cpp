@@ -36,6 +36,7 @@ TileConfig default_tile_config(uint32_t n) {
     c.m = static_cast<uint32_t>(env_int("LQCS_TILE_BITS", 12));
     c.L = static_cast<uint32_t>(env_int("LQCS_TILE_LOW", 5));
     c.inner = static_cast<uint32_t>(env_int("LQCS_TILE_INNER", 2));
+    c.reg = env_int("LQCS_TILE_REG", 1) != 0;
     c.m = std::max<uint32_t>(kTileMinBits, std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n));
     c.L = std::min<uint32_t>(std::min(c.L, c.m), kTileMinBits);   // column bits come from the thread index
     if (c.m - c.L > kTileMaxHigh) c.L = c.m - kTileMaxHigh;
@@ -152,6 +153,31 @@ uint32_t deposit(uint32_t v, const std::vector<uint32_t>& sorted_pos) {
     return v;
 }
 
+bool is_diagonal(const std::vector<cd>& m, uint64_t dim) {
+    for (uint64_t r = 0; r < dim; ++r)
+        for (uint64_t c = 0; c < dim; ++c)
+            if (r != c && m[r * dim + c] != cd{0, 0}) return false;
+    return true;
+}
+
+// Dense or diagonal op of matrix m on local targets lt, local controls lcmask.
+LocalOp matrix_op(const std::vector<cd>& m, const std::vector<uint32_t>& lt, uint32_t lcmask,
+                  uint64_t gcmask) {
+    LocalOp op;
+    const uint64_t dim = uint64_t{1} << lt.size();
+    op.lt = lt;
+    op.lmask = lcmask;
+    op.gcmask = gcmask;
+    if (is_diagonal(m, dim)) {
+        op.kind = kTileDiag;
+        for (uint64_t i = 0; i < dim; ++i) op.m.push_back(m[i * dim + i]);
+    } else {
+        op.kind = kTileDense;
+        op.m = m;
+    }
+    return op;
+}
+
 // Group enumeration of an op on a 2^m tile: the positions spread over (ascending), the
 // group count, and the per-iteration slot parts sw(deposit(j * threads) | lcmask).
 void set_groups(TileOp& op, std::vector<uint32_t> pos, uint32_t lcmask, uint32_t m) {
@@ -165,90 +191,34 @@ void set_groups(TileOp& op, std::vector<uint32_t> pos, uint32_t lcmask, uint32_t
         op.dhi[j] = static_cast<uint16_t>(tile_swizzle(deposit(j * kTileThreads, pos) | lcmask));
 }
 
-// Dense or diagonal op of matrix m on local target positions lt (matrix local order).
-TileOp make_matrix_op(const std::vector<cd>& m, const std::vector<uint32_t>& lt, uint32_t lcmask,
-                      uint64_t gcmask, std::vector<cd>& arena, uint32_t tile_bits) {
-    TileOp op{};
-    const uint32_t k = static_cast<uint32_t>(lt.size());
-    const uint64_t dim = uint64_t{1} << k;
-    bool diag = true;
-    for (uint64_t r = 0; r < dim && diag; ++r)
-        for (uint64_t c = 0; c < dim; ++c)
-            if (r != c && m[r * dim + c] != cd{0, 0}) { diag = false; break; }
-    op.kind = diag ? kTileDiag : kTileDense;
-    op.k = static_cast<uint8_t>(k);
-    op.gcmask = gcmask;
-    for (uint64_t l = 0; l < dim; ++l) {
-        uint32_t o = 0;
-        for (uint32_t j = 0; j < k; ++j)
-            if ((l >> j) & 1) o |= 1u << lt[j];
-        op.soff[l] = static_cast<uint16_t>(tile_swizzle(o));
-    }
-    std::vector<uint32_t> fixed = lt;
-    for (uint32_t b = 0; b < 32; ++b)
-        if ((lcmask >> b) & 1) fixed.push_back(b);
-    set_groups(op, fixed, lcmask, tile_bits);
-    op.mat_off = static_cast<uint32_t>(arena.size());
-    if (diag) {
-        for (uint64_t i = 0; i < dim; ++i) arena.push_back(m[i * dim + i]);
-    } else {
-        arena.insert(arena.end(), m.begin(), m.end());
-    }
-    return op;
-}
-
 }  // namespace
 
-void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
-                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena) {
+std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
+                                    const TileConfig& cfg, uint32_t max_select) {
     LocalMap lm{cfg.L, item.hbits};
-    pass = TilePass{};
-    pass.L = cfg.L;
-    pass.h = static_cast<uint32_t>(item.hbits.size());
-    pass.m = cfg.L + pass.h;
-    for (uint32_t i = 0; i < pass.h; ++i) pass.hbits[i] = item.hbits[i];
-    const size_t first = ops_out.size();
-
-    // inner fusion: greedy blocks over gates whose qubits are all local; any other gate
-    // closes the blocks it touches and is emitted on its own
+    std::vector<LocalOp> out;
+    // inner fusion: greedy blocks of at most cfg.inner local qubits (targets and local
+    // controls) and at most max_select out-of-tile controls; any other gate closes the
+    // blocks it touches and is emitted on its own
     struct Open {
-        std::vector<uint32_t> qubits;   // global, sorted
+        std::vector<uint32_t> qubits;   // local part, global numbering, sorted
+        std::vector<uint32_t> sel;      // out-of-tile controls, sorted
         std::vector<uint32_t> gates;
         bool alive = true;
     };
     std::vector<Open> open;
     std::vector<int> owner(64, -1);
-    auto emit_block = [&](Open& b) {
-        if (!b.alive) return;
-        b.alive = false;
-        for (uint32_t q : b.qubits) owner[q] = -1;
-        std::vector<uint32_t> lt;
-        for (uint32_t q : b.qubits) lt.push_back(static_cast<uint32_t>(lm.local(q)));
-        FusedBlock fb;
-        fb.qubits = b.qubits;
-        fb.gates = b.gates;
-        const std::vector<cd> m = block_matrix(fb, gates);
-        ops_out.push_back(make_matrix_op(m, lt, 0, 0, arena, pass.m));
-    };
     auto emit_single = [&](const GateDesc& g) {
         if (is_phase_gate(g)) {
-            TileOp op{};
+            LocalOp op;
             op.kind = kTilePhase;
-            std::vector<uint32_t> fixed;
-            uint32_t lmask = 0;
             for (uint32_t q : g.qubits) {
                 const int l = lm.local(q);
-                if (l >= 0) {
-                    lmask |= 1u << l;
-                    fixed.push_back(static_cast<uint32_t>(l));
-                } else {
-                    op.gcmask |= uint64_t{1} << q;
-                }
+                if (l >= 0) op.lmask |= 1u << l;
+                else op.gcmask |= uint64_t{1} << q;
             }
-            set_groups(op, fixed, lmask, pass.m);
-            op.mat_off = static_cast<uint32_t>(arena.size());
-            arena.push_back(g.base_matrix()[3]);
-            ops_out.push_back(op);
+            op.m.push_back(g.base_matrix()[3]);
+            out.push_back(std::move(op));
             return;
         }
         std::vector<uint32_t> lt;
@@ -262,35 +232,106 @@ void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const 
             if (l >= 0) lc |= 1u << l;
             else gc |= uint64_t{1} << q;
         }
-        ops_out.push_back(make_matrix_op(g.base_matrix(), lt, lc, gc, arena, pass.m));
+        out.push_back(matrix_op(g.base_matrix(), lt, lc, gc));
+    };
+    auto emit_block = [&](Open& b) {
+        if (!b.alive) return;
+        b.alive = false;
+        for (uint32_t q : b.qubits) owner[q] = -1;
+        if (b.gates.size() == 1) {   // keeps the cheaper single-gate encodings (controls, X)
+            emit_single(gates[b.gates[0]]);
+            return;
+        }
+        std::vector<uint32_t> lt;
+        for (uint32_t q : b.qubits) lt.push_back(static_cast<uint32_t>(lm.local(q)));
+        FusedBlock fb;
+        fb.qubits = b.qubits;
+        if (b.sel.empty()) {
+            fb.gates = b.gates;
+            out.push_back(matrix_op(block_matrix(fb, gates), lt, 0, 0));
+            return;
+        }
+        // one matrix per value s of the out-of-tile controls (bit i of s = qubit sel[i]): a
+        // gate acts, without those controls, where all of its own are 1 and is the identity
+        // elsewhere
+        const uint32_t c = static_cast<uint32_t>(b.sel.size());
+        const uint64_t dim = uint64_t{1} << lt.size();
+        std::vector<std::vector<cd>> mats;
+        bool diag = true;
+        for (uint32_t sv = 0; sv < (1u << c); ++sv) {
+            std::vector<GateDesc> red;
+            for (uint32_t gi : b.gates) {
+                const GateDesc& g = gates[gi];
+                GateDesc r = g;
+                r.qubits.clear();
+                r.n_controls = 0;
+                bool on = true;
+                for (uint32_t k = 0; k < g.n_controls; ++k) {
+                    const uint32_t q = g.controls()[k];
+                    if (lm.local(q) >= 0) {
+                        r.qubits.push_back(q);
+                        ++r.n_controls;
+                    } else {
+                        const auto it = std::find(b.sel.begin(), b.sel.end(), q);
+                        on &= ((sv >> (it - b.sel.begin())) & 1u) != 0;
+                    }
+                }
+                for (uint32_t j = 0; j < g.base_qubits(); ++j) r.qubits.push_back(g.targets()[j]);
+                if (on) red.push_back(std::move(r));
+            }
+            fb.gates.clear();
+            for (uint32_t i = 0; i < red.size(); ++i) fb.gates.push_back(i);
+            mats.push_back(block_matrix(fb, red));
+            diag &= is_diagonal(mats.back(), dim);
+        }
+        LocalOp op;
+        op.kind = diag ? kTileDiag : kTileDense;
+        op.lt = lt;
+        op.sel = b.sel;
+        for (const std::vector<cd>& m : mats) {
+            if (diag) {
+                for (uint64_t i = 0; i < dim; ++i) op.m.push_back(m[i * dim + i]);
+            } else {
+                op.m.insert(op.m.end(), m.begin(), m.end());
+            }
+        }
+        out.push_back(std::move(op));
     };
 
     for (uint32_t gi : item.gates) {
         const GateDesc& g = gates[gi];
-        bool all_local = !is_phase_gate(g);
-        for (uint32_t q : g.qubits) all_local &= lm.local(q) >= 0;
-        if (cfg.inner < 2 || !all_local || g.qubits.size() > cfg.inner) {
-            for (uint32_t q : g.qubits)
+        std::vector<uint32_t> part, sel;   // local qubits; out-of-tile controls
+        for (uint32_t q : g.qubits) (lm.local(q) >= 0 ? part : sel).push_back(q);
+        std::sort(part.begin(), part.end());
+        std::sort(sel.begin(), sel.end());
+        if (cfg.inner < 2 || is_phase_gate(g) || part.size() > cfg.inner || sel.size() > max_select) {
+            for (uint32_t q : part)
                 if (owner[q] >= 0) emit_block(open[owner[q]]);
             emit_single(g);
             continue;
         }
         std::vector<int> touched;
-        for (uint32_t q : g.qubits)
+        for (uint32_t q : part)
             if (owner[q] >= 0 && std::find(touched.begin(), touched.end(), owner[q]) == touched.end())
                 touched.push_back(owner[q]);
-        std::vector<uint32_t> uni(g.qubits.begin(), g.qubits.end());
-        for (int b : touched) uni.insert(uni.end(), open[b].qubits.begin(), open[b].qubits.end());
+        std::vector<uint32_t> uni = part, usel = sel;
+        for (int b : touched) {
+            uni.insert(uni.end(), open[b].qubits.begin(), open[b].qubits.end());
+            usel.insert(usel.end(), open[b].sel.begin(), open[b].sel.end());
+        }
         std::sort(uni.begin(), uni.end());
         uni.erase(std::unique(uni.begin(), uni.end()), uni.end());
+        std::sort(usel.begin(), usel.end());
+        usel.erase(std::unique(usel.begin(), usel.end()), usel.end());
         Open nb;
-        if (uni.size() > cfg.inner) {
+        if (uni.size() > cfg.inner || usel.size() > max_select) {
             for (int b : touched) emit_block(open[b]);
-            nb.qubits.assign(g.qubits.begin(), g.qubits.end());
-            std::sort(nb.qubits.begin(), nb.qubits.end());
+            nb.qubits = part;
+            nb.sel = sel;
             nb.gates = {gi};
         } else {
             nb.qubits = uni;
+            nb.sel = usel;
             for (int b : touched) {
                 nb.gates.insert(nb.gates.end(), open[b].gates.begin(), open[b].gates.end());
                 open[b].alive = false;
@@ -303,10 +344,314 @@ void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const 
         open.push_back(std::move(nb));
     }
     for (Open& b : open) emit_block(b);
+    return out;
+}
+
+void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
+                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena) {
+    pass = TilePass{};
+    pass.L = cfg.L;
+    pass.h = static_cast<uint32_t>(item.hbits.size());
+    pass.m = cfg.L + pass.h;
+    for (uint32_t i = 0; i < pass.h; ++i) pass.hbits[i] = item.hbits[i];
+    const size_t first = ops_out.size();
+    for (const LocalOp& lo : pass_local_ops(item, gates, cfg, 0)) {
+        TileOp op{};
+        op.kind = lo.kind;
+        op.gcmask = lo.gcmask;
+        op.mat_off = static_cast<uint32_t>(arena.size());
+        arena.insert(arena.end(), lo.m.begin(), lo.m.end());
+        if (lo.kind == kTilePhase) {
+            std::vector<uint32_t> fixed;
+            for (uint32_t b = 0; b < 32; ++b)
+                if ((lo.lmask >> b) & 1) fixed.push_back(b);
+            set_groups(op, fixed, lo.lmask, pass.m);
+        } else {
+            const uint32_t k = static_cast<uint32_t>(lo.lt.size());
+            op.k = static_cast<uint8_t>(k);
+            for (uint32_t l = 0; l < (1u << k); ++l) {
+                uint32_t o = 0;
+                for (uint32_t j = 0; j < k; ++j)
+                    if ((l >> j) & 1) o |= 1u << lo.lt[j];
+                op.soff[l] = static_cast<uint16_t>(tile_swizzle(o));
+            }
+            std::vector<uint32_t> fixed = lo.lt;
+            for (uint32_t b = 0; b < 32; ++b)
+                if ((lo.lmask >> b) & 1) fixed.push_back(b);
+            set_groups(op, fixed, lo.lmask, pass.m);
+        }
+        ops_out.push_back(op);
+    }
     pass.n_ops = static_cast<uint32_t>(ops_out.size() - first);
     pass.kmax = 1;
     for (size_t i = first; i < ops_out.size(); ++i)
         if (ops_out[i].kind != kTilePhase) pass.kmax = std::max<uint32_t>(pass.kmax, ops_out[i].k);
+}
+
+// ------------------------------------------------------------------ register passes
+
+namespace {
+
+constexpr uint32_t kLaneBits = 5;
+
+uint32_t target_mask(const LocalOp& o) {
+    uint32_t t = 0;
+    for (uint32_t b : o.lt) t |= 1u << b;
+    return t;
+}
+
+// Tile bits an op uses off the diagonal (dense targets) and on it (controls, phase bits,
+// diagonal targets).  Two ops commute when every bit they share is diagonal in both.
+struct Use {
+    uint32_t nd = 0, dg = 0;
+};
+Use op_use(const LocalOp& o) {
+    Use u;
+    if (o.kind == kTileDense) u.nd = target_mask(o);
+    else if (o.kind == kTileDiag) u.dg = target_mask(o);
+    u.dg |= o.lmask;
+    return u;
+}
+
+// Scan of the pending ops under register set S: every op that commutes with all skipped
+// ops before it and whose dense targets are register bits is applied.  Returns the count;
+// with `emitted` the applied ops move there (in order) and `pending` keeps the rest.
+size_t scan(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
+            std::vector<uint32_t>& pending, uint32_t S, std::vector<uint32_t>* emitted) {
+    uint32_t busy_nd = 0, busy_dg = 0;
+    size_t cnt = 0;
+    std::vector<uint32_t> rest;
+    for (uint32_t i : pending) {
+        const Use& u = use[i];
+        const bool blocked = (u.nd & (busy_nd | busy_dg)) != 0 || (u.dg & busy_nd) != 0;
+        const bool fits = ops[i].kind != kTileDense || (target_mask(ops[i]) & ~S) == 0;
+        if (!blocked && fits) {
+            ++cnt;
+            if (emitted) emitted->push_back(i);
+        } else {
+            busy_nd |= u.nd;
+            busy_dg |= u.dg;
+            if (emitted) rest.push_back(i);
+        }
+    }
+    if (emitted) pending = std::move(rest);
+    return cnt;
+}
+
+// Dense ops of `pending` whose targets all lie in S (a tie-break: later use of a layout).
+size_t covered(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pending, uint32_t S) {
+    size_t c = 0;
+    for (uint32_t i : pending)
+        if (ops[i].kind == kTileDense && (target_mask(ops[i]) & ~S) == 0) ++c;
+    return c;
+}
+
+// Layout of register set S on an m-bit tile.  Thread bits ascending, except that when the
+// low five are not tile bits 0..4 the first three are picked with distinct residues mod 3:
+// tile_swizzle sends 1 << b to slot bit (b mod 3), so then the 8 lanes of a quarter warp hit
+// 8 different 16-byte bank groups in a remap.
+RegLayout make_layout(uint32_t S, uint32_t m) {
+    RegLayout ly{};
+    std::vector<uint32_t> rb, tb;
+    for (uint32_t b = 0; b < m; ++b) ((S >> b) & 1 ? rb : tb).push_back(b);
+    if ((S & ((1u << kLaneBits) - 1u)) != 0) {
+        std::vector<uint32_t> first, rest;
+        uint32_t seen = 0;
+        for (uint32_t b : tb) {
+            if (first.size() < 3 && !((seen >> (b % 3)) & 1)) {
+                first.push_back(b);
+                seen |= 1u << (b % 3);
+            } else {
+                rest.push_back(b);
+            }
+        }
+        tb = first;
+        tb.insert(tb.end(), rest.begin(), rest.end());
+    }
+    for (uint32_t i = 0; i < kRegBits; ++i) {
+        ly.rpos[i] = static_cast<uint8_t>(rb[i]);
+        ly.rsw[i] = static_cast<uint16_t>(tile_swizzle(1u << rb[i]));
+    }
+    for (uint32_t i = 0; i < tb.size(); ++i) {
+        ly.tpos[i] = static_cast<uint8_t>(tb[i]);
+        ly.tsw[i] = static_cast<uint16_t>(tile_swizzle(1u << tb[i]));
+    }
+    return ly;
+}
+
+bool is_x(const std::vector<cd>& m) {
+    return m.size() == 4 && m[0] == cd{0, 0} && m[1] == cd{1, 0} && m[2] == cd{1, 0} &&
+           m[3] == cd{0, 0};
+}
+
+// Register sets of size kRegBits inside `allowed` that contain `must`, best first by
+// (ops applied now, dense ops covered later, usable as the final layout).
+uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
+                    std::vector<uint32_t>& pending, uint32_t must, uint32_t allowed, uint32_t m) {
+    uint32_t best = 0;
+    size_t best_now = 0, best_later = 0;
+    bool best_final = false, have = false;
+    const uint32_t lanes = (1u << kLaneBits) - 1u;
+    for (uint32_t S = 0; S < (1u << m); ++S) {
+        if (__builtin_popcount(S) != static_cast<int>(kRegBits) || (S & must) != must ||
+            (S & ~allowed) != 0)
+            continue;
+        const size_t now = scan(ops, use, pending, S, nullptr);
+        const size_t later = covered(ops, pending, S);
+        const bool fin = (S & lanes) == 0;
+        if (!have || now > best_now || (now == best_now && later > best_later) ||
+            (now == best_now && later == best_later && fin && !best_final)) {
+            have = true;
+            best = S;
+            best_now = now;
+            best_later = later;
+            best_final = fin;
+        }
+    }
+    return best;
+}
+
+}  // namespace
+
+namespace {
+
+bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates,
+                        const TileConfig& cfg, uint32_t max_select, RegPass& pass,
+                        std::vector<RegOp>& ops_out, std::vector<RegLayout>& layouts_out,
+                        std::vector<cd>& mats_out) {
+    const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
+    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select);
+    for (const LocalOp& o : ops)
+        if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : 4u)) return false;
+    std::vector<Use> use;
+    for (const LocalOp& o : ops) use.push_back(op_use(o));
+
+    std::vector<RegOp> rec;
+    std::vector<RegLayout> lays;
+    std::vector<uint32_t> lay_sets;
+    std::vector<cd> mats;
+    auto layout_index = [&](uint32_t S) {
+        for (size_t i = 0; i < lay_sets.size(); ++i)
+            if (lay_sets[i] == S) return static_cast<uint32_t>(i);
+        lay_sets.push_back(S);
+        lays.push_back(make_layout(S, m));
+        return static_cast<uint32_t>(lay_sets.size() - 1);
+    };
+    auto emit = [&](const LocalOp& o, const RegLayout& ly, uint32_t S) {
+        int ridx[32], tidx[32];
+        for (uint32_t i = 0; i < kRegBits; ++i) ridx[ly.rpos[i]] = static_cast<int>(i);
+        for (uint32_t i = 0; i < m - kRegBits; ++i) tidx[ly.tpos[i]] = static_cast<int>(i);
+        RegOp r{};
+        r.gcmask = o.gcmask;
+        r.mat_off = static_cast<uint32_t>(mats.size());
+        r.nsel = static_cast<uint8_t>(o.sel.size());
+        for (size_t i = 0; i < o.sel.size(); ++i) r.selq[i] = static_cast<uint8_t>(o.sel[i]);
+        for (uint32_t b = 0; b < m; ++b) {
+            if (!((o.lmask >> b) & 1)) continue;
+            if ((S >> b) & 1) r.rcmask = static_cast<uint8_t>(r.rcmask | (1u << ridx[b]));
+            else r.tcmask = static_cast<uint16_t>(r.tcmask | (1u << tidx[b]));
+        }
+        const uint32_t k = static_cast<uint32_t>(o.lt.size());
+        r.k = static_cast<uint8_t>(k);
+        if (o.kind == kTilePhase) {
+            r.kind = kRegPhase;
+            mats.push_back(o.m[0]);
+        } else if (o.kind == kTileDiag) {
+            r.kind = kRegDiag;
+            for (uint32_t j = 0; j < k; ++j) {
+                const uint32_t b = o.lt[j];
+                r.loc[j] = static_cast<uint8_t>((S >> b) & 1 ? ridx[b] : (0x80 | tidx[b]));
+            }
+            mats.insert(mats.end(), o.m.begin(), o.m.end());
+        } else {
+            uint32_t tm = 0;
+            for (uint32_t b : o.lt) tm |= 1u << ridx[b];
+            r.code = static_cast<uint8_t>(tm);
+            if (k == 1 && o.sel.empty() && is_x(o.m)) {
+                r.kind = kRegSwapX;
+            } else {
+                r.kind = kRegDense;
+                // matrix index bit q <-> the q-th lowest register target
+                std::vector<uint32_t> pos(k);
+                for (uint32_t j = 0; j < k; ++j) {
+                    const uint32_t rb = static_cast<uint32_t>(ridx[o.lt[j]]);
+                    pos[j] = static_cast<uint32_t>(__builtin_popcount(tm & ((1u << rb) - 1u)));
+                }
+                const uint32_t D = 1u << k;
+                std::vector<uint32_t> perm(D);
+                for (uint32_t l = 0; l < D; ++l) {
+                    uint32_t p = 0;
+                    for (uint32_t j = 0; j < k; ++j)
+                        if ((l >> j) & 1) p |= 1u << pos[j];
+                    perm[l] = p;
+                }
+                std::vector<cd> pm(D * D);
+                for (size_t blk = 0; blk < o.m.size(); blk += D * D) {   // per selector value
+                    for (uint32_t rr = 0; rr < D; ++rr)
+                        for (uint32_t cc = 0; cc < D; ++cc)
+                            pm[perm[rr] * D + perm[cc]] = o.m[blk + rr * D + cc];
+                    mats.insert(mats.end(), pm.begin(), pm.end());
+                }
+            }
+        }
+        rec.push_back(r);
+    };
+
+    const uint32_t all = (1u << m) - 1u;
+    const uint32_t high = all & ~((1u << kLaneBits) - 1u);
+    std::vector<uint32_t> pending(ops.size());
+    for (uint32_t i = 0; i < ops.size(); ++i) pending[i] = i;
+    // the first layout loads the tile: lanes on tile bits 0..4 keep the loads coalesced
+    uint32_t S = choose_set(ops, use, pending, 0, high, m);
+    uint32_t cur = layout_index(S);
+    while (true) {
+        std::vector<uint32_t> applied;
+        scan(ops, use, pending, S, &applied);
+        for (uint32_t i : applied) emit(ops[i], lays[cur], S);
+        if (pending.empty()) break;
+        S = choose_set(ops, use, pending, target_mask(ops[pending.front()]), all, m);
+        cur = layout_index(S);
+        RegOp r{};
+        r.kind = kRegRemap;
+        r.code = static_cast<uint8_t>(cur);
+        rec.push_back(r);
+    }
+    if ((S & ((1u << kLaneBits) - 1u)) != 0) {
+        // the store wants lanes on tile bits 0..4 again
+        RegOp r{};
+        r.kind = kRegRemap;
+        r.code = static_cast<uint8_t>(layout_index(all & ~((1u << (m - kRegBits)) - 1u)));
+        rec.push_back(r);
+    }
+    if (rec.size() > kRegMaxRecords || lays.size() > kRegMaxLayouts || mats.size() > kRegMaxMatrix)
+        return false;
+    pass = RegPass{};
+    pass.L = cfg.L;
+    pass.h = static_cast<uint32_t>(item.hbits.size());
+    pass.m = m;
+    for (uint32_t i = 0; i < pass.h; ++i) pass.hbits[i] = item.hbits[i];
+    pass.n_ops = static_cast<uint32_t>(rec.size());
+    pass.n_layouts = static_cast<uint32_t>(lays.size());
+    pass.n_mat = static_cast<uint32_t>(mats.size());
+    ops_out.insert(ops_out.end(), rec.begin(), rec.end());
+    layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());
+    mats_out.insert(mats_out.end(), mats.begin(), mats.end());
+    return true;
+}
+
+}  // namespace
+
+bool lower_pass_reg(const PlanItem& item, const std::vector<GateDesc>& gates,
+                    const TileConfig& cfg, RegPass& pass, std::vector<RegOp>& ops_out,
+                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out) {
+    const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
+    if (m < kRegMinBits || m > kRegMaxBits || item.hbits.size() > kTileMaxHigh) return false;
+    // fewer selector qubits when the matrices of a pass outgrow their shared-memory stage
+    for (int sel = static_cast<int>(kRegMaxSelect); sel >= 0; --sel)
+        if (lower_pass_reg_sel(item, gates, cfg, static_cast<uint32_t>(sel), pass, ops_out,
+                               layouts_out, mats_out))
+            return true;
+    return false;
 }
 
 }  // namespace lqcs_b200

@@ -12,6 +12,7 @@ struct TileConfig {
     uint32_t m = 12;       // tile bits (2^m amplitudes in shared memory)
     uint32_t L = 5;        // low qubits always in the tile
     uint32_t inner = 2;    // widest dense operation fused inside a pass
+    bool reg = true;       // register tile kernel where the pass fits it
 };
 TileConfig default_tile_config(uint32_t n);
 
@@ -26,8 +27,35 @@ struct PlanItem {
 std::vector<PlanItem> plan_tiles(const std::vector<GateDesc>& gates, uint32_t n,
                                  const TileConfig& cfg);
 
+// One operation of a pass in tile-local bits, before it is encoded for a kernel.
+struct LocalOp {
+    uint8_t kind = kTileDense;      // kTileDense, kTileDiag or kTilePhase
+    std::vector<uint32_t> lt;       // targets, matrix local order (none for a phase)
+    uint32_t lmask = 0;             // local controls, or the local bits of a phase
+    uint64_t gcmask = 0;            // controls / phase bits outside the tile
+    std::vector<uint32_t> sel;      // out-of-tile qubits selecting one of 2^|sel| matrices
+    std::vector<cd> m;              // dense: 2^k x 2^k, diagonal: 2^k, phase: the factor;
+                                    // with sel, one such block per selector value
+};
+
+// The operations of one pass in program order, neighbouring gates fused into blocks of at
+// most cfg.inner local qubits.  A block may take gates controlled by up to max_select
+// qubits outside the tile: those bits are constant over a tile, so the block becomes one
+// matrix per value of them, picked per tile.
+std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
+                                    const TileConfig& cfg, uint32_t max_select);
+
 // Append the tile operations of one pass to ops_out (matrices to arena) and fill `pass`.
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
                 TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena);
+
+// Register-tile encoding of one pass: the operations scheduled over a sequence of register
+// layouts (greedy: each layout applies every pending operation it can, the next one is the
+// register set that applies the most), with a remap record between layouts.  Returns false
+// when the pass does not fit the register kernel (tile size, a dense operation of more than
+// kRegMaxK targets, record / layout / matrix limits); nothing is appended then.
+bool lower_pass_reg(const PlanItem& item, const std::vector<GateDesc>& gates,
+                    const TileConfig& cfg, RegPass& pass, std::vector<RegOp>& ops_out,
+                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out);
 
 }  // namespace lqcs_b200

@@ -1,6 +1,6 @@
-"""GPU parity of the shared-memory tile passes (fusion_mode 4, the default from 12 qubits)
-and of the greedy dense-block path (fusion_mode 1) against the oracle, for every gate type
-and several tile shapes."""
+"""GPU parity of the tile passes (fusion_mode 4, the default from 12 qubits) — register
+kernel and shared-memory kernel — and of the greedy dense-block path (fusion_mode 1)
+against the oracle, for every gate type and several tile shapes."""
 import os
 
 import numpy as np
@@ -19,13 +19,14 @@ GREEDY = 1
 
 @pytest.fixture
 def tile_env():
-    keys = ("LQCS_TILE_BITS", "LQCS_TILE_LOW", "LQCS_TILE_INNER")
+    keys = ("LQCS_TILE_BITS", "LQCS_TILE_LOW", "LQCS_TILE_INNER", "LQCS_TILE_REG")
     saved = {k: os.environ.get(k) for k in keys}
 
-    def set_cfg(m, low, inner):
+    def set_cfg(m, low, inner, reg=1):
         os.environ["LQCS_TILE_BITS"] = str(m)
         os.environ["LQCS_TILE_LOW"] = str(low)
         os.environ["LQCS_TILE_INNER"] = str(inner)
+        os.environ["LQCS_TILE_REG"] = str(reg)
 
     yield set_cfg
     for k, v in saved.items():
@@ -43,10 +44,19 @@ def run(qc, mode, init=None):
     return sv.to_numpy()
 
 
+def kernel_kinds(qc):
+    """Profile kinds of a tile-mode program's device ops (6 shared-memory, 7 register pass)."""
+    prog = lq.simulator.CompiledCircuit(qc, True, 0, TILE)
+    sv = lq.Statevector(qc.num_qubits())
+    return [r["kind"] for r in prog.profile(sv)]
+
+
+@pytest.mark.parametrize("reg", [1, 0])
 @pytest.mark.parametrize("n", [6, 8, 11, 13])
-@pytest.mark.parametrize("cfg", [(12, 5, 2), (11, 5, 1), (13, 5, 3), (10, 6, 4), (12, 4, 2)])
-def test_tile_passes_every_gate_type(port, tile_env, n, cfg):
-    tile_env(*cfg)
+@pytest.mark.parametrize("cfg", [(12, 5, 2), (11, 5, 1), (13, 5, 3), (10, 6, 4), (12, 4, 2),
+                                 (9, 5, 2)])
+def test_tile_passes_every_gate_type(port, tile_env, n, cfg, reg):
+    tile_env(*cfg, reg)
     init = W.gaussian_state(n, seed=n + cfg[0])
     qc = random_circuit(n, 90, seed=31 * n + cfg[2], max_controls=4, max_unitary=4)
     want = port.run_statevector(qc, fuse=False, state=init)
@@ -54,9 +64,10 @@ def test_tile_passes_every_gate_type(port, tile_env, n, cfg):
     assert np.max(np.abs(got - want)) < TOL
 
 
+@pytest.mark.parametrize("reg", [1, 0])
 @pytest.mark.parametrize("inner", [1, 2, 3, 4])
-def test_tile_brickwork_and_qft_vs_reference(ref, tile_env, inner):
-    tile_env(12, 5, inner)
+def test_tile_brickwork_and_qft_vs_reference(ref, tile_env, inner, reg):
+    tile_env(12, 5, inner, reg)
     qc = W.brickwork(18, 12, seed=77)
     want = ref.run_statevector(qc, fuse=True)
     assert np.max(np.abs(run(qc, TILE) - want)) < TOL
@@ -66,8 +77,9 @@ def test_tile_brickwork_and_qft_vs_reference(ref, tile_env, inner):
     assert np.max(np.abs(run(q, TILE, init) - want)) < TOL
 
 
-def test_tile_barrier_and_wide_gates(port, tile_env):
-    tile_env(12, 5, 2)
+@pytest.mark.parametrize("reg", [1, 0])
+def test_tile_barrier_and_wide_gates(port, tile_env, reg):
+    tile_env(12, 5, 2, reg)
     n = 14
     init = W.gaussian_state(n, seed=8)
     qc = random_circuit(n, 40, seed=5)
@@ -91,9 +103,10 @@ def test_greedy_blocks_at_tile_sizes(port, n):
         assert np.max(np.abs(sv.to_numpy() - want)) < TOL
 
 
-def test_tile_batch_of_states(port, tile_env):
+@pytest.mark.parametrize("reg", [1, 0])
+def test_tile_batch_of_states(port, tile_env, reg):
     """Tile passes walk a batch of states (gridDim.y)."""
-    tile_env(12, 5, 2)
+    tile_env(12, 5, 2, reg)
     from litequantumcomputingsimulator_b200 import _native as N
     import ctypes as C
     n, batch = 13, 3
@@ -111,3 +124,48 @@ def test_tile_batch_of_states(port, tile_env):
     for b in range(batch):
         want = port.run_statevector(qc, fuse=False, state=inits[b])
         assert np.max(np.abs(out[b << n:(b + 1) << n] - want)) < TOL
+
+
+@pytest.mark.parametrize("m", [9, 10, 11, 12, 13])
+def test_register_kernel_runs_the_passes(ref, tile_env, m):
+    """With inner fusion <= 3 every pass of a brickwork fits the register kernel; with the
+    register kernel off they all run in shared memory; both agree with the reference."""
+    qc = W.brickwork(16, 10, seed=3)
+    want = ref.run_statevector(qc, fuse=True)
+    tile_env(m, 5, 2, 1)
+    kinds = kernel_kinds(qc)
+    assert kinds and all(k == 7 for k in kinds)
+    assert np.max(np.abs(run(qc, TILE) - want)) < TOL
+    tile_env(m, 5, 2, 0)
+    assert all(k == 6 for k in kernel_kinds(qc))
+    assert np.max(np.abs(run(qc, TILE) - want)) < TOL
+
+
+def test_register_kernel_controls_phases_and_diagonals(port, tile_env):
+    """Controls and phase bits on register bits, thread bits and out-of-tile qubits; diagonal
+    blocks; X gates on register bits (swap path)."""
+    tile_env(12, 5, 2, 1)
+    n = 16
+    rng = np.random.default_rng(12)
+    qc = lq.QuantumCircuit(n)
+    for _ in range(160):
+        kind = int(rng.integers(7))
+        q = [int(x) for x in rng.permutation(n)[:4]]
+        if kind == 0:
+            qc.u(*rng.uniform(0, 6.3, 3), q[0])
+        elif kind == 1:
+            qc.cx(q[0], q[1])
+        elif kind == 2:
+            qc.ccx(q[0], q[1], q[2])
+        elif kind == 3:
+            qc.cp(float(rng.uniform(0, 6.3)), q[0], q[1])
+        elif kind == 4:
+            qc.rzz(float(rng.uniform(0, 6.3)), q[0], q[1])
+        elif kind == 5:
+            qc.x(q[0])
+        else:
+            qc.cry(float(rng.uniform(0, 6.3)), q[0], q[1])
+    init = W.gaussian_state(n, seed=2)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    assert 7 in kernel_kinds(qc)
+    assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
