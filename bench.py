@@ -61,6 +61,37 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp64_peak(torch, device):
+    """FP64 throughput of a library DGEMM on this GPU (TFLOP/s, best of 10): the FP64
+    roofline denominator, measured in the run like the HBM copy peak."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(3):
+        torch.matmul(a, b)
+    best = None
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+def ncu_traffic():
+    """DRAM bytes per state amplitude of each kernel, from ncu captures (profiles/)."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return {}
+    d = json.loads(p.read_text())
+    return {k: v for k, v in d.items() if isinstance(v, dict) and "bytes_per_amplitude" in v}
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -288,22 +319,42 @@ def main():
     prof = prog.profile(sv)
     by_kernel = {}
     for r in prof:
-        k = by_kernel.setdefault(r["kernel"], {"ms": 0.0, "bytes": 0.0, "launches": 0})
+        k = by_kernel.setdefault(r["kernel"], {"ms": 0.0, "bytes": 0.0, "flops": 0.0, "launches": 0})
         k["ms"] += r["ms"]
         k["bytes"] += r["alg_bytes"]
+        k["flops"] += r["alg_flops"]
         k["launches"] += 1
     dom_name, dom = max(by_kernel.items(), key=lambda kv: kv[1]["ms"])
     prof_total = sum(v["ms"] for v in by_kernel.values())
-    achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                "traffic": None, "launches": dom["launches"],
-                "share": dom["ms"] / prof_total,
-                "alg_bytes_per_launch": dom["bytes"] / dom["launches"],
-                "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
-                                "share": round(v["ms"] / prof_total, 4),
-                                "gbs": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1)}
-                            for k, v in by_kernel.items()}}
+    fp64 = fp64_peak(torch, device)
+    gbs = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+    tfs = dom["flops"] / (dom["ms"] / 1e3) / 1e12
+    hbm_frac, fp64_frac = gbs / hbm_peak, tfs / fp64
+    base_kernel = dom_name.split("<")[0]
+    traffic = None
+    t = ncu_traffic().get(base_kernel)
+    if t:
+        traffic = t["bytes_per_amplitude"] * float(1 << n)   # per launch, scaled to 2^n
+    # the bound is the resource the kernel's algorithmic work needs most of
+    if fp64_frac > hbm_frac:
+        roofline = {"bound": "fp64", "achieved": tfs, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": fp64_frac, "peak_kind": "measured in this run (DGEMM 4096^3, best of 10)"}
+    else:
+        roofline = {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_frac, "peak_kind": peak_kind}
+    roofline.update({
+        "kernel": dom_name, "traffic": traffic, "launches": dom["launches"],
+        "share": dom["ms"] / prof_total,
+        "alg_bytes_per_launch": dom["bytes"] / dom["launches"],
+        "alg_flops_per_launch": dom["flops"] / dom["launches"],
+        "hbm": {"achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": hbm_frac, "peak_kind": peak_kind},
+        "fp64": {"achieved_tflops": tfs, "peak_tflops": fp64, "frac": fp64_frac,
+                 "peak_kind": "measured in this run (DGEMM 4096^3, best of 10)"},
+        "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                        "share": round(v["ms"] / prof_total, 4),
+                        "gbs": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1),
+                        "tflops": round(v["flops"] / (v["ms"] / 1e3) / 1e12, 2)}
+                    for k, v in by_kernel.items()}})
 
     extras = {}
     if not args.no_extras and rank == 0:
@@ -433,18 +484,34 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
         out["qft_error"] = str(ex)
 
     # noisy trajectories: 26-qubit brickwork depth 20, depolarizing 1e-3 after each U3,
-    # 1e-2 on both qubits after each CX, amplitude damping 1e-3 per qubit per layer; one
-    # resident batch of 64 trajectories (a bounded sample of the 1024-trajectory run)
+    # 1e-2 on both qubits after each CX, amplitude damping 1e-3 per qubit per layer; up to 64
+    # resident per batch.  Fused driver: 128 trajectories (2 batches, a bounded sample of the
+    # 1024-trajectory run); gate-by-gate driver: 16 trajectories, for the comparison.
     try:
         tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+        warm = W.brickwork(12, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3))
         sim = lq.StatevectorSimulator(seed=404, max_resident=64)
-        sim.run_registers(W.brickwork(10, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3)), 8)
+        sim.run_registers(warm, 8)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim.run_registers(tq, 64)
+        fused_regs = sim.run_registers(tq, 128)
         dt = time.perf_counter() - t0
-        out["trajectories_26q_per_s"] = 64 / dt
-        out["trajectories_26q_sample"] = "64 trajectories resident at once (1 GiB each), host-timed"
+        out["trajectories_26q_per_s"] = 128 / dt
+        out["trajectories_26q_sample"] = ("128 trajectories, 64 resident per batch (1 GiB each), "
+                                          "fused driver, host-timed")
+        os.environ["LQCS_TRAJ_FUSED"] = "0"
+        try:
+            plain = lq.StatevectorSimulator(seed=404, max_resident=16)
+            plain.run_registers(warm, 8)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            plain_regs = plain.run_registers(tq, 16)
+            dtp = time.perf_counter() - t0
+        finally:
+            os.environ.pop("LQCS_TRAJ_FUSED", None)
+        out["trajectories_26q_plain_per_s"] = 16 / dtp
+        out["trajectories_26q_fused_speedup"] = (128 / dt) / (16 / dtp)
+        out["trajectories_26q_same_registers"] = bool((fused_regs[:16] == plain_regs).all())
     except Exception as ex:  # noqa: BLE001
         out["trajectories_error"] = str(ex)
 

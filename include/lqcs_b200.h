@@ -194,6 +194,8 @@ typedef struct lqcs_op_profile {
     uint32_t n_controls;
     double device_ms;
     double alg_bytes;       /* 32 * 2^n * f: amplitudes the operation can change, read+written */
+    double alg_flops;       /* FP64 flops executed: 8 per complex multiply-add (dense blocks),
+                               6 per complex multiply (diagonals, phases), 0 for permutations */
 } lqcs_op_profile;
 
 int lqcs_program_apply_profiled(lqcs_state* st, const lqcs_program* prog, uint64_t cap,

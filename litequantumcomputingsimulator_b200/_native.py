@@ -94,6 +94,7 @@ class OpProfile(C.Structure):
         ("n_controls", C.c_uint32),
         ("device_ms", C.c_double),
         ("alg_bytes", C.c_double),
+        ("alg_flops", C.c_double),
     ]
 
 

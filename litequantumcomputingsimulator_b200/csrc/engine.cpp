@@ -254,7 +254,8 @@ static Program assemble_tiles(const std::vector<GateDesc>& gates, uint32_t n,
         if (cfg.reg) {
             RegPass rp;
             const size_t o0 = p.reg_ops.size(), l0 = p.reg_layouts.size(), m0 = p.reg_mats.size();
-            if (lower_pass_reg(it, gates, cfg, rp, p.reg_ops, p.reg_layouts, p.reg_mats)) {
+            if (lower_pass_reg(it, gates, cfg, rp, p.reg_ops, p.reg_layouts, p.reg_mats,
+                               &op.tile_flops)) {
                 p.reg_op_off.push_back(o0);
                 p.reg_lay_off.push_back(l0);
                 p.reg_mat_off.push_back(m0);
@@ -267,7 +268,7 @@ static Program assemble_tiles(const std::vector<GateDesc>& gates, uint32_t n,
         }
         TilePass tp;
         p.pass_op_off.push_back(p.tile_ops.size());
-        lower_pass(it, gates, cfg, tp, p.tile_ops, p.tile_mats);
+        lower_pass(it, gates, cfg, tp, p.tile_ops, p.tile_mats, &op.tile_flops);
         op.pass_index = static_cast<uint32_t>(p.passes.size());
         p.passes.push_back(tp);
         ops.push_back(std::move(op));
@@ -324,6 +325,45 @@ static Program compile_learned(const std::vector<GateDesc>& gates, uint32_t n,
     }
     best_prog.build(std::move(best_ops), stream);
     return best_prog;
+}
+
+bool compile_slots(const std::vector<GateDesc>& gates, uint32_t n,
+                   const std::vector<std::vector<std::array<cd, 4>>>& slots, cudaStream_t stream,
+                   Program& out) {
+    if (n < kRegMinBits) return false;
+    const TileConfig cfg = default_tile_config(n);
+    Program p;
+    std::vector<DevOp> ops;
+    for (const PlanItem& it : plan_tiles(gates, n, cfg)) {
+        if (!it.is_pass) {
+            if (gates[it.gate].slot) return false;
+            ops.push_back(lower_gate(gates[it.gate], n));
+            continue;
+        }
+        bool has_slot = false;
+        for (uint32_t gi : it.gates) has_slot |= gates[gi].slot;
+        DevOp op;
+        op.kind = OpKind::TILE;
+        op.k = static_cast<uint32_t>(it.hbits.size());
+        op.targets = it.hbits;
+        op.src_gates = static_cast<uint32_t>(it.gates.size());
+        op.alg_fraction = 1.0;
+        op.reg_tile = true;
+        RegPass rp;
+        const size_t o0 = p.reg_ops.size(), l0 = p.reg_layouts.size(), m0 = p.reg_mats.size();
+        if (!lower_pass_reg(it, gates, cfg, rp, p.reg_ops, p.reg_layouts, p.reg_mats,
+                            &op.tile_flops, has_slot ? &slots : nullptr))
+            return false;
+        p.reg_op_off.push_back(o0);
+        p.reg_lay_off.push_back(l0);
+        p.reg_mat_off.push_back(m0);
+        op.pass_index = static_cast<uint32_t>(p.reg_passes.size());
+        p.reg_passes.push_back(rp);
+        ops.push_back(std::move(op));
+    }
+    p.build(std::move(ops), stream);
+    out = std::move(p);
+    return true;
 }
 
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
@@ -460,6 +500,7 @@ void program_profile(lqcs_state& st, const lqcs_program& p, uint64_t cap, lqcs_o
         r.n_controls = static_cast<uint32_t>(__builtin_popcountll(op.cmask));
         r.device_ms = ms;
         r.alg_bytes = 32.0 * static_cast<double>(st.len()) * op.alg_fraction * st.batch;
+        r.alg_flops = op_flops_per_amp(op) * static_cast<double>(st.len()) * st.batch;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     *n_out = nops;

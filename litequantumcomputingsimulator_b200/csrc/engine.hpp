@@ -82,6 +82,13 @@ uint32_t default_fusion_width();
 // Compile a list of unitary gates to a Program (fused or gate by gate).
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
                 cudaStream_t stream);
+
+// Tile-pass program for a batch whose noise slots (GateDesc::slot) take per-state matrices
+// (slots[b][slot_id] for state b).  False when some pass does not fit the register kernel
+// or a slot would run outside a pass; `out` is then unusable.
+bool compile_slots(const std::vector<GateDesc>& gates, uint32_t n,
+                   const std::vector<std::vector<std::array<cd, 4>>>& slots, cudaStream_t stream,
+                   Program& out);
 std::vector<FusedBlock> plan(const std::vector<GateDesc>& gates, uint32_t n,
                              const FusionConfig& fc);
 

@@ -389,6 +389,19 @@ double gate_alg_fraction(const GateDesc& g) {
     return ctrl;
 }
 
+double op_flops_per_amp(const DevOp& op) {
+    switch (op.kind) {
+        case OpKind::K1Q: return (op.diag1 ? 6.0 : 16.0) * op.alg_fraction;
+        case OpKind::PHASE: return 6.0 * op.alg_fraction;
+        case OpKind::DENSE: return 8.0 * std::ldexp(1.0, static_cast<int>(op.k)) * op.alg_fraction;
+        case OpKind::DIAG: return 6.0 * op.alg_fraction;
+        case OpKind::PERM: return 0.0;
+        case OpKind::PAULI: return 16.0 * op.alg_fraction;
+        case OpKind::TILE: return op.tile_flops;
+    }
+    return 0.0;
+}
+
 // ------------------------------------------------------------------ lowering
 
 DevOp lower_gate(const GateDesc& g, uint32_t n) {

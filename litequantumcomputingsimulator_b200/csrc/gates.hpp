@@ -37,6 +37,11 @@ struct GateDesc {
     std::string pauli;                   // PAULI_ROTATION
     uint32_t clbit = 0;                  // MEASURE
     std::vector<std::array<cd, 4>> kraus;  // KRAUS
+    // Engine-internal: a noise slot of a trajectory batch — a one-qubit UNITARY whose 2x2
+    // matrix differs per state (slot_id indexes the per-state tables); never specialised
+    // as a phase, diagonal or X.
+    bool slot = false;
+    uint32_t slot_id = 0;
 
     uint32_t base_qubits() const;        // Gate::base_qubits (src/circuit/gate.cpp:27-49)
     bool is_unitary() const;             // not Measure / Reset / Barrier / Kraus
@@ -90,10 +95,16 @@ struct DevOp {
     // TILE: index of the pass in the program's shared-memory or register pass list
     uint32_t pass_index = 0;
     bool reg_tile = false;
+    double tile_flops = 0.0;             // TILE: FP64 flops per state amplitude of the pass
     // bookkeeping
     uint32_t src_gates = 1;              // source gates merged into this op
     double alg_fraction = 1.0;           // fraction of amplitudes it can change
 };
+
+// FP64 flops per state amplitude an op executes: 8 per complex multiply-add of a dense
+// 2^k block row (8 * 2^k), 6 per complex multiply of a diagonal or phase, none for
+// permutations; scaled by the fraction of amplitudes the op touches.
+double op_flops_per_amp(const DevOp& op);
 
 // Kind number of an op in profiles and cost-model features: the OpKind, or 7 for a tile
 // pass run by the register kernel.

@@ -281,7 +281,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
     }
     {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(mats);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(
+            mats + static_cast<uint64_t>(blockIdx.y) * p.mat_stride);   // this state's matrices
         uint32_t* dst = reinterpret_cast<uint32_t*>(smat);
         for (uint32_t w = threadIdx.x; w < p.n_mat * 4u; w += kT) dst[w] = src[w];
         src = reinterpret_cast<const uint32_t*>(ops);
@@ -308,6 +309,19 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             for (int u = 0; u < kE; ++u)
                 v[u] = __ldcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
                                    ((u & 8) ? g3 : 0)));
+        }
+        // Start the HBM reads of this CTA's next tile into L2 while this one computes, so
+        // its loads above hit L2 on the next iteration.  Thread r < 2^h takes the row of
+        // high-bit pattern r: 2^L contiguous amplitudes, 16 B * 2^L from a 16 B boundary.
+        if (threadIdx.x < (1u << p.h) && tid + gridDim.x < p.n_tiles) {
+            uint64_t nb = (tid + gridDim.x) << p.L;
+            for (uint32_t i = 0; i < p.h; ++i) {
+                nb = insert_zero_bit(nb, shbits[i]);
+                if ((threadIdx.x >> i) & 1u) nb |= uint64_t{1} << shbits[i];
+            }
+            const double2* row = s + nb;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(16u << p.L)
+                         : "memory");
         }
         uint32_t cur = 0;
         for (uint32_t o = 0; o < p.n_ops; ++o) {

@@ -114,6 +114,7 @@ struct RegPass {
     uint64_t batch_stride;
     uint32_t m, L, h;
     uint32_t n_ops, n_layouts, n_mat;
+    uint32_t mat_stride;      // double2 between the matrices of consecutive states (0: shared)
     uint32_t hbits[kTileMaxHigh];
 };
 

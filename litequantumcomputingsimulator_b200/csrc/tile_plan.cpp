@@ -18,7 +18,7 @@ namespace lqcs_b200 {
 namespace {
 
 bool is_phase_gate(const GateDesc& g) {
-    if (!g.is_unitary() || g.base_qubits() != 1) return false;
+    if (g.slot || !g.is_unitary() || g.base_qubits() != 1) return false;
     if (g.type == LQCS_GATE_PAULI_ROTATION) return false;
     const std::vector<cd> m = g.base_matrix();
     return m[1] == cd{0, 0} && m[2] == cd{0, 0} && m[0] == cd{1, 0};
@@ -162,13 +162,14 @@ bool is_diagonal(const std::vector<cd>& m, uint64_t dim) {
 
 // Dense or diagonal op of matrix m on local targets lt, local controls lcmask.
 LocalOp matrix_op(const std::vector<cd>& m, const std::vector<uint32_t>& lt, uint32_t lcmask,
-                  uint64_t gcmask) {
+                  uint64_t gcmask, bool variant) {
     LocalOp op;
     const uint64_t dim = uint64_t{1} << lt.size();
     op.lt = lt;
     op.lmask = lcmask;
     op.gcmask = gcmask;
-    if (is_diagonal(m, dim)) {
+    op.variant = variant;
+    if (!variant && is_diagonal(m, dim)) {
         op.kind = kTileDiag;
         for (uint64_t i = 0; i < dim; ++i) op.m.push_back(m[i * dim + i]);
     } else {
@@ -191,12 +192,36 @@ void set_groups(TileOp& op, std::vector<uint32_t> pos, uint32_t lcmask, uint32_t
         op.dhi[j] = static_cast<uint16_t>(tile_swizzle(deposit(j * kTileThreads, pos) | lcmask));
 }
 
+bool is_x(const std::vector<cd>& m) {
+    return m.size() == 4 && m[0] == cd{0, 0} && m[1] == cd{1, 0} && m[2] == cd{1, 0} &&
+           m[3] == cd{0, 0};
+}
+
 }  // namespace
 
+double local_op_flops(const LocalOp& o, bool x_free) {
+    const double frac = std::ldexp(1.0, -(__builtin_popcount(o.lmask) + __builtin_popcountll(o.gcmask)));
+    if (o.kind != kTileDense) return 6.0 * frac;
+    if (x_free && !o.variant && o.lt.size() == 1 && o.sel.empty() && is_x(o.m)) return 0.0;
+    return 8.0 * std::ldexp(1.0, static_cast<int>(o.lt.size())) * frac;
+}
+
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
-                                    const TileConfig& cfg, uint32_t max_select) {
+                                    const TileConfig& cfg, uint32_t max_select,
+                                    const std::vector<std::array<cd, 4>>* slot_mats) {
     LocalMap lm{cfg.L, item.hbits};
     std::vector<LocalOp> out;
+    // a noise slot takes this state's matrix (identity when no table is given)
+    auto resolved = [&](const GateDesc& g) {
+        GateDesc r = g;
+        if (g.slot) {
+            r.type = LQCS_GATE_UNITARY;
+            r.mat.assign(4, cd{0, 0});
+            r.mat[0] = r.mat[3] = 1.0;
+            if (slot_mats) r.mat.assign((*slot_mats)[g.slot_id].begin(), (*slot_mats)[g.slot_id].end());
+        }
+        return r;
+    };
     // inner fusion: greedy blocks of at most cfg.inner local qubits (targets and local
     // controls) and at most max_select out-of-tile controls; any other gate closes the
     // blocks it touches and is emitted on its own
@@ -232,7 +257,7 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
             if (l >= 0) lc |= 1u << l;
             else gc |= uint64_t{1} << q;
         }
-        out.push_back(matrix_op(g.base_matrix(), lt, lc, gc));
+        out.push_back(matrix_op(resolved(g).base_matrix(), lt, lc, gc, g.slot));
     };
     auto emit_block = [&](Open& b) {
         if (!b.alive) return;
@@ -246,9 +271,15 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
         for (uint32_t q : b.qubits) lt.push_back(static_cast<uint32_t>(lm.local(q)));
         FusedBlock fb;
         fb.qubits = b.qubits;
+        bool variant = false;
+        for (uint32_t gi : b.gates) variant |= gates[gi].slot;
         if (b.sel.empty()) {
-            fb.gates = b.gates;
-            out.push_back(matrix_op(block_matrix(fb, gates), lt, 0, 0));
+            std::vector<GateDesc> res;
+            for (uint32_t gi : b.gates) {
+                fb.gates.push_back(static_cast<uint32_t>(res.size()));
+                res.push_back(resolved(gates[gi]));
+            }
+            out.push_back(matrix_op(block_matrix(fb, res), lt, 0, 0, variant));
             return;
         }
         // one matrix per value s of the out-of-tile controls (bit i of s = qubit sel[i]): a
@@ -261,7 +292,7 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
         for (uint32_t sv = 0; sv < (1u << c); ++sv) {
             std::vector<GateDesc> red;
             for (uint32_t gi : b.gates) {
-                const GateDesc& g = gates[gi];
+                const GateDesc g = resolved(gates[gi]);
                 GateDesc r = g;
                 r.qubits.clear();
                 r.n_controls = 0;
@@ -282,12 +313,13 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
             fb.gates.clear();
             for (uint32_t i = 0; i < red.size(); ++i) fb.gates.push_back(i);
             mats.push_back(block_matrix(fb, red));
-            diag &= is_diagonal(mats.back(), dim);
+            diag &= !variant && is_diagonal(mats.back(), dim);
         }
         LocalOp op;
         op.kind = diag ? kTileDiag : kTileDense;
         op.lt = lt;
         op.sel = b.sel;
+        op.variant = variant;
         for (const std::vector<cd>& m : mats) {
             if (diag) {
                 for (uint64_t i = 0; i < dim; ++i) op.m.push_back(m[i * dim + i]);
@@ -348,14 +380,17 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
 }
 
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
-                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena) {
+                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena,
+                double* flops_per_amp) {
     pass = TilePass{};
     pass.L = cfg.L;
     pass.h = static_cast<uint32_t>(item.hbits.size());
     pass.m = cfg.L + pass.h;
     for (uint32_t i = 0; i < pass.h; ++i) pass.hbits[i] = item.hbits[i];
     const size_t first = ops_out.size();
+    double flops = 0.0;
     for (const LocalOp& lo : pass_local_ops(item, gates, cfg, 0)) {
+        flops += local_op_flops(lo, false);
         TileOp op{};
         op.kind = lo.kind;
         op.gcmask = lo.gcmask;
@@ -383,6 +418,7 @@ void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const 
         ops_out.push_back(op);
     }
     pass.n_ops = static_cast<uint32_t>(ops_out.size() - first);
+    if (flops_per_amp) *flops_per_amp = flops;
     pass.kmax = 1;
     for (size_t i = first; i < ops_out.size(); ++i)
         if (ops_out[i].kind != kTilePhase) pass.kmax = std::max<uint32_t>(pass.kmax, ops_out[i].k);
@@ -479,11 +515,6 @@ RegLayout make_layout(uint32_t S, uint32_t m) {
     return ly;
 }
 
-bool is_x(const std::vector<cd>& m) {
-    return m.size() == 4 && m[0] == cd{0, 0} && m[1] == cd{1, 0} && m[2] == cd{1, 0} &&
-           m[3] == cd{0, 0};
-}
-
 // Register sets of size kRegBits inside `allowed` that contain `must`, best first by
 // (ops applied now, dense ops covered later, usable as the final layout).
 uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
@@ -515,21 +546,97 @@ uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use
 
 namespace {
 
+// Matrix data of op o in layout (ly, S): dense matrices re-indexed so that matrix bit q is
+// the q-th lowest register target (one block per selector value), diagonals and phase
+// factors as they are.  X operations (swaps) have none.
+void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vector<cd>& mats) {
+    if (o.kind == kTilePhase || o.kind == kTileDiag) {
+        mats.insert(mats.end(), o.m.begin(), o.m.end());
+        return;
+    }
+    const uint32_t k = static_cast<uint32_t>(o.lt.size());
+    if (k == 1 && !o.variant && o.sel.empty() && is_x(o.m)) return;
+    int ridx[32];
+    for (uint32_t i = 0; i < kRegBits; ++i) ridx[ly.rpos[i]] = static_cast<int>(i);
+    uint32_t tm = 0;
+    for (uint32_t b : o.lt) tm |= 1u << ridx[b];
+    (void)S;
+    std::vector<uint32_t> pos(k);
+    for (uint32_t j = 0; j < k; ++j) {
+        const uint32_t rb = static_cast<uint32_t>(ridx[o.lt[j]]);
+        pos[j] = static_cast<uint32_t>(__builtin_popcount(tm & ((1u << rb) - 1u)));
+    }
+    const uint32_t D = 1u << k;
+    std::vector<uint32_t> perm(D);
+    for (uint32_t l = 0; l < D; ++l) {
+        uint32_t p = 0;
+        for (uint32_t j = 0; j < k; ++j)
+            if ((l >> j) & 1) p |= 1u << pos[j];
+        perm[l] = p;
+    }
+    std::vector<cd> pm(D * D);
+    for (size_t blk = 0; blk < o.m.size(); blk += D * D) {   // per selector value
+        for (uint32_t rr = 0; rr < D; ++rr)
+            for (uint32_t cc = 0; cc < D; ++cc) pm[perm[rr] * D + perm[cc]] = o.m[blk + rr * D + cc];
+        mats.insert(mats.end(), pm.begin(), pm.end());
+    }
+}
+
+// The record of op o in layout (ly, S); its matrices start at mat_off.
+RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m, uint32_t mat_off) {
+    int ridx[32], tidx[32];
+    for (uint32_t i = 0; i < kRegBits; ++i) ridx[ly.rpos[i]] = static_cast<int>(i);
+    for (uint32_t i = 0; i < m - kRegBits; ++i) tidx[ly.tpos[i]] = static_cast<int>(i);
+    RegOp r{};
+    r.gcmask = o.gcmask;
+    r.mat_off = mat_off;
+    r.nsel = static_cast<uint8_t>(o.sel.size());
+    for (size_t i = 0; i < o.sel.size(); ++i) r.selq[i] = static_cast<uint8_t>(o.sel[i]);
+    for (uint32_t b = 0; b < m; ++b) {
+        if (!((o.lmask >> b) & 1)) continue;
+        if ((S >> b) & 1) r.rcmask = static_cast<uint8_t>(r.rcmask | (1u << ridx[b]));
+        else r.tcmask = static_cast<uint16_t>(r.tcmask | (1u << tidx[b]));
+    }
+    const uint32_t k = static_cast<uint32_t>(o.lt.size());
+    r.k = static_cast<uint8_t>(k);
+    if (o.kind == kTilePhase) {
+        r.kind = kRegPhase;
+    } else if (o.kind == kTileDiag) {
+        r.kind = kRegDiag;
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t b = o.lt[j];
+            r.loc[j] = static_cast<uint8_t>((S >> b) & 1 ? ridx[b] : (0x80 | tidx[b]));
+        }
+    } else {
+        uint32_t tm = 0;
+        for (uint32_t b : o.lt) tm |= 1u << ridx[b];
+        r.code = static_cast<uint8_t>(tm);
+        r.kind = (k == 1 && !o.variant && o.sel.empty() && is_x(o.m)) ? kRegSwapX : kRegDense;
+    }
+    return r;
+}
+
+bool same_shape(const LocalOp& a, const LocalOp& b) {
+    return a.kind == b.kind && a.lt == b.lt && a.lmask == b.lmask && a.gcmask == b.gcmask &&
+           a.sel == b.sel && a.m.size() == b.m.size() && a.variant == b.variant;
+}
+
 bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates,
                         const TileConfig& cfg, uint32_t max_select, RegPass& pass,
                         std::vector<RegOp>& ops_out, std::vector<RegLayout>& layouts_out,
-                        std::vector<cd>& mats_out) {
+                        std::vector<cd>& mats_out, double* flops_per_amp,
+                        const std::vector<std::vector<std::array<cd, 4>>>* state_slots) {
     const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
-    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select);
+    const std::vector<std::array<cd, 4>>* slots0 =
+        state_slots && !state_slots->empty() ? &(*state_slots)[0] : nullptr;
+    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select, slots0);
     for (const LocalOp& o : ops)
         if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : 4u)) return false;
     std::vector<Use> use;
     for (const LocalOp& o : ops) use.push_back(op_use(o));
 
-    std::vector<RegOp> rec;
     std::vector<RegLayout> lays;
     std::vector<uint32_t> lay_sets;
-    std::vector<cd> mats;
     auto layout_index = [&](uint32_t S) {
         for (size_t i = 0; i < lay_sets.size(); ++i)
             if (lay_sets[i] == S) return static_cast<uint32_t>(i);
@@ -537,66 +644,8 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
         lays.push_back(make_layout(S, m));
         return static_cast<uint32_t>(lay_sets.size() - 1);
     };
-    auto emit = [&](const LocalOp& o, const RegLayout& ly, uint32_t S) {
-        int ridx[32], tidx[32];
-        for (uint32_t i = 0; i < kRegBits; ++i) ridx[ly.rpos[i]] = static_cast<int>(i);
-        for (uint32_t i = 0; i < m - kRegBits; ++i) tidx[ly.tpos[i]] = static_cast<int>(i);
-        RegOp r{};
-        r.gcmask = o.gcmask;
-        r.mat_off = static_cast<uint32_t>(mats.size());
-        r.nsel = static_cast<uint8_t>(o.sel.size());
-        for (size_t i = 0; i < o.sel.size(); ++i) r.selq[i] = static_cast<uint8_t>(o.sel[i]);
-        for (uint32_t b = 0; b < m; ++b) {
-            if (!((o.lmask >> b) & 1)) continue;
-            if ((S >> b) & 1) r.rcmask = static_cast<uint8_t>(r.rcmask | (1u << ridx[b]));
-            else r.tcmask = static_cast<uint16_t>(r.tcmask | (1u << tidx[b]));
-        }
-        const uint32_t k = static_cast<uint32_t>(o.lt.size());
-        r.k = static_cast<uint8_t>(k);
-        if (o.kind == kTilePhase) {
-            r.kind = kRegPhase;
-            mats.push_back(o.m[0]);
-        } else if (o.kind == kTileDiag) {
-            r.kind = kRegDiag;
-            for (uint32_t j = 0; j < k; ++j) {
-                const uint32_t b = o.lt[j];
-                r.loc[j] = static_cast<uint8_t>((S >> b) & 1 ? ridx[b] : (0x80 | tidx[b]));
-            }
-            mats.insert(mats.end(), o.m.begin(), o.m.end());
-        } else {
-            uint32_t tm = 0;
-            for (uint32_t b : o.lt) tm |= 1u << ridx[b];
-            r.code = static_cast<uint8_t>(tm);
-            if (k == 1 && o.sel.empty() && is_x(o.m)) {
-                r.kind = kRegSwapX;
-            } else {
-                r.kind = kRegDense;
-                // matrix index bit q <-> the q-th lowest register target
-                std::vector<uint32_t> pos(k);
-                for (uint32_t j = 0; j < k; ++j) {
-                    const uint32_t rb = static_cast<uint32_t>(ridx[o.lt[j]]);
-                    pos[j] = static_cast<uint32_t>(__builtin_popcount(tm & ((1u << rb) - 1u)));
-                }
-                const uint32_t D = 1u << k;
-                std::vector<uint32_t> perm(D);
-                for (uint32_t l = 0; l < D; ++l) {
-                    uint32_t p = 0;
-                    for (uint32_t j = 0; j < k; ++j)
-                        if ((l >> j) & 1) p |= 1u << pos[j];
-                    perm[l] = p;
-                }
-                std::vector<cd> pm(D * D);
-                for (size_t blk = 0; blk < o.m.size(); blk += D * D) {   // per selector value
-                    for (uint32_t rr = 0; rr < D; ++rr)
-                        for (uint32_t cc = 0; cc < D; ++cc)
-                            pm[perm[rr] * D + perm[cc]] = o.m[blk + rr * D + cc];
-                    mats.insert(mats.end(), pm.begin(), pm.end());
-                }
-            }
-        }
-        rec.push_back(r);
-    };
-
+    // schedule: (op, layout) in application order, remaps as (-1, new layout)
+    std::vector<std::pair<int, uint32_t>> seq;
     const uint32_t all = (1u << m) - 1u;
     const uint32_t high = all & ~((1u << kLaneBits) - 1u);
     std::vector<uint32_t> pending(ops.size());
@@ -607,24 +656,45 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     while (true) {
         std::vector<uint32_t> applied;
         scan(ops, use, pending, S, &applied);
-        for (uint32_t i : applied) emit(ops[i], lays[cur], S);
+        for (uint32_t i : applied) seq.emplace_back(static_cast<int>(i), cur);
         if (pending.empty()) break;
         S = choose_set(ops, use, pending, target_mask(ops[pending.front()]), all, m);
         cur = layout_index(S);
-        RegOp r{};
-        r.kind = kRegRemap;
-        r.code = static_cast<uint8_t>(cur);
-        rec.push_back(r);
+        seq.emplace_back(-1, cur);
     }
-    if ((S & ((1u << kLaneBits) - 1u)) != 0) {
-        // the store wants lanes on tile bits 0..4 again
-        RegOp r{};
-        r.kind = kRegRemap;
-        r.code = static_cast<uint8_t>(layout_index(all & ~((1u << (m - kRegBits)) - 1u)));
-        rec.push_back(r);
+    if ((S & ((1u << kLaneBits) - 1u)) != 0)   // the store wants lanes on tile bits 0..4 again
+        seq.emplace_back(-1, layout_index(all & ~((1u << (m - kRegBits)) - 1u)));
+
+    // records and the first state's matrices
+    std::vector<RegOp> rec;
+    std::vector<cd> mats;
+    for (const auto& [i, l] : seq) {
+        if (i < 0) {
+            RegOp r{};
+            r.kind = kRegRemap;
+            r.code = static_cast<uint8_t>(l);
+            rec.push_back(r);
+            continue;
+        }
+        rec.push_back(make_record(ops[i], lays[l], lay_sets[l], m, static_cast<uint32_t>(mats.size())));
+        append_matrices(ops[i], lays[l], lay_sets[l], mats);
     }
     if (rec.size() > kRegMaxRecords || lays.size() > kRegMaxLayouts || mats.size() > kRegMaxMatrix)
         return false;
+    const size_t n_mat = mats.size();
+    // every further state: same records, its own slot matrices
+    if (state_slots) {
+        for (size_t b = 1; b < state_slots->size(); ++b) {
+            const std::vector<LocalOp> ob = pass_local_ops(item, gates, cfg, max_select, &(*state_slots)[b]);
+            if (ob.size() != ops.size()) return false;
+            for (size_t i = 0; i < ops.size(); ++i)
+                if (!same_shape(ops[i], ob[i])) return false;
+            const size_t before = mats.size();
+            for (const auto& [i, l] : seq)
+                if (i >= 0) append_matrices(ob[i], lays[l], lay_sets[l], mats);
+            if (mats.size() - before != n_mat) return false;
+        }
+    }
     pass = RegPass{};
     pass.L = cfg.L;
     pass.h = static_cast<uint32_t>(item.hbits.size());
@@ -632,10 +702,15 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     for (uint32_t i = 0; i < pass.h; ++i) pass.hbits[i] = item.hbits[i];
     pass.n_ops = static_cast<uint32_t>(rec.size());
     pass.n_layouts = static_cast<uint32_t>(lays.size());
-    pass.n_mat = static_cast<uint32_t>(mats.size());
+    pass.n_mat = static_cast<uint32_t>(n_mat);
+    pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());
     layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());
     mats_out.insert(mats_out.end(), mats.begin(), mats.end());
+    if (flops_per_amp) {
+        *flops_per_amp = 0.0;
+        for (const LocalOp& o : ops) *flops_per_amp += local_op_flops(o, true);
+    }
     return true;
 }
 
@@ -643,13 +718,15 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
 
 bool lower_pass_reg(const PlanItem& item, const std::vector<GateDesc>& gates,
                     const TileConfig& cfg, RegPass& pass, std::vector<RegOp>& ops_out,
-                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out) {
+                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out,
+                    double* flops_per_amp,
+                    const std::vector<std::vector<std::array<cd, 4>>>* state_slots) {
     const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
     if (m < kRegMinBits || m > kRegMaxBits || item.hbits.size() > kTileMaxHigh) return false;
     // fewer selector qubits when the matrices of a pass outgrow their shared-memory stage
     for (int sel = static_cast<int>(kRegMaxSelect); sel >= 0; --sel)
         if (lower_pass_reg_sel(item, gates, cfg, static_cast<uint32_t>(sel), pass, ops_out,
-                               layouts_out, mats_out))
+                               layouts_out, mats_out, flops_per_amp, state_slots))
             return true;
     return false;
 }

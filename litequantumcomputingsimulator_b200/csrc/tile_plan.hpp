@@ -34,6 +34,7 @@ struct LocalOp {
     uint32_t lmask = 0;             // local controls, or the local bits of a phase
     uint64_t gcmask = 0;            // controls / phase bits outside the tile
     std::vector<uint32_t> sel;      // out-of-tile qubits selecting one of 2^|sel| matrices
+    bool variant = false;           // contains a noise slot: the matrices differ per state
     std::vector<cd> m;              // dense: 2^k x 2^k, diagonal: 2^k, phase: the factor;
                                     // with sel, one such block per selector value
 };
@@ -43,19 +44,29 @@ struct LocalOp {
 // qubits outside the tile: those bits are constant over a tile, so the block becomes one
 // matrix per value of them, picked per tile.
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
-                                    const TileConfig& cfg, uint32_t max_select);
+                                    const TileConfig& cfg, uint32_t max_select,
+                                    const std::vector<std::array<cd, 4>>* slot_mats = nullptr);
 
 // Append the tile operations of one pass to ops_out (matrices to arena) and fill `pass`.
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
-                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena);
+                TilePass& pass, std::vector<TileOp>& ops_out, std::vector<cd>& arena,
+                double* flops_per_amp = nullptr);
 
 // Register-tile encoding of one pass: the operations scheduled over a sequence of register
 // layouts (greedy: each layout applies every pending operation it can, the next one is the
 // register set that applies the most), with a remap record between layouts.  Returns false
 // when the pass does not fit the register kernel (tile size, a dense operation of more than
 // kRegMaxK targets, record / layout / matrix limits); nothing is appended then.
+// With state_slots (one table of noise-slot matrices per state of a batch) the records are
+// shared and the matrices are stored once per state, n_mat apart (pass.mat_stride).
 bool lower_pass_reg(const PlanItem& item, const std::vector<GateDesc>& gates,
                     const TileConfig& cfg, RegPass& pass, std::vector<RegOp>& ops_out,
-                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out);
+                    std::vector<RegLayout>& layouts_out, std::vector<cd>& mats_out,
+                    double* flops_per_amp = nullptr,
+                    const std::vector<std::vector<std::array<cd, 4>>>* state_slots = nullptr);
+
+// FP64 flops per state amplitude one pass operation executes (op_flops_per_amp's
+// conventions); x_free: an uncontrolled-by-selector X runs as a register swap.
+double local_op_flops(const LocalOp& o, bool x_free);
 
 }  // namespace lqcs_b200

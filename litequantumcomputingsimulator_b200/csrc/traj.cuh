@@ -16,6 +16,8 @@ struct TrajDecide {
     uint32_t uniform_index;   // index of this event's uniform within a shot
     uint32_t n_ops;           // mode 0: Kraus operators (2x2 each, device memory)
     const double2* ops;
+    const int* forced;        // mode 0, optional (device, per state): branch >= 0 known in
+                              // advance -> K_branch applied unnormalised, no reduction
 };
 
 // Device scratch for a resident batch of R trajectories.
@@ -28,7 +30,8 @@ struct TrajScratch {
 };
 
 // rdm of qubit q per state -> branch per state (uniform u[(first+b)*per_shot+j]) ->
-// K/sqrt(p) applied per state.
+// K/sqrt(p) applied per state.  States need not be normalised: probabilities are taken
+// relative to the state's norm and the chosen branch leaves the state normalised.
 void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
                        const TrajDecide& d, const double* d_uniforms, uint64_t first,
                        uint64_t per_shot, TrajScratch& s);

@@ -61,7 +61,9 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* out_row, uint
 // Per state: rho of qubit q = {sum |a0|^2, sum |a1|^2, Re sum a0 conj(a1), Im ...}
 // partials layout [state][value][block]
 __global__ void __launch_bounds__(kThreads) k_b_rdm1(const double2* __restrict__ st, uint64_t len,
-                                                     uint32_t q, double* __restrict__ partials) {
+                                                     uint32_t q, double* __restrict__ partials,
+                                                     const int* __restrict__ skip) {
+    if (skip && skip[blockIdx.y] >= 0) return;   // branch known: no reduction needed
     const double2* s = st + static_cast<uint64_t>(blockIdx.y) * len;
     const uint64_t half = len >> 1, qb = uint64_t{1} << q;
     double v[4] = {0, 0, 0, 0};
@@ -82,26 +84,36 @@ __global__ void __launch_bounds__(kThreads) k_b_rdm1(const double2* __restrict__
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
 // One thread per state: sum the partials, then decide.
-// mode 0 (Kraus): probabilities Tr(K_i rho K_i^dagger), first i with u < cumulative p
-//                 (p <= 0 skipped, last non-zero branch as fallback), mats[b] = K_i/sqrt(p_i),
-//                 flag[b] = 1 (0 only when every probability is zero: nothing is applied).
-// mode 1 (measure/reset): p1 = rho11, outcome = u < p1, scale 1/sqrt(keep); the clbit of
-//                 the register is set or cleared (measure only).
+// The state need not be normalised: with t = Tr(rho) = rho00 + rho11,
+// mode 0 (Kraus): probabilities p_i = Tr(K_i rho K_i^dagger) / t, first i with
+//                 u < cumulative p (p <= 0 skipped, last non-zero branch as fallback),
+//                 mats[b] = K_i / sqrt(p_i t), flag[b] = 1 (0 only when every probability is
+//                 zero: nothing is applied).  A forced branch (forced[b] >= 0) is applied as
+//                 K_i, without reduction or normalisation.
+// mode 1 (measure/reset): p1 = rho11 / t, outcome = u < p1, scale 1/sqrt(rho_oo); the clbit
+//                 of the register is set or cleared (measure only).
 __global__ void k_b_decide(const double* __restrict__ partials, uint32_t nb, uint32_t batch,
                            TrajDecide d, const double* __restrict__ uniforms, uint64_t first,
                            uint64_t per_shot, double2* __restrict__ mats, int* __restrict__ flag,
                            double* __restrict__ scale, uint64_t* __restrict__ regs) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= batch) return;
+    if (d.mode == 0 && d.forced && d.forced[b] >= 0) {
+        const double2* k = d.ops + 4 * d.forced[b];
+        for (int e = 0; e < 4; ++e) mats[4 * b + e] = k[e];
+        flag[b] = 1;
+        return;
+    }
     double r[4] = {0, 0, 0, 0};
     const double* row = partials + static_cast<uint64_t>(b) * 4 * nb;
     for (int k = 0; k < 4; ++k)
         for (uint32_t j = 0; j < nb; ++j) r[k] += row[k * nb + j];
     const double u = uniforms[(first + b) * per_shot + d.uniform_index];
+    const double tr = r[0] + r[1];
     if (d.mode == 1) {
-        const double p1 = r[1];
+        const double p1 = r[1] / tr;
         const int outcome = u < p1 ? 1 : 0;
-        const double keep = outcome ? p1 : 1.0 - p1;
+        const double keep = outcome ? r[1] : r[0];
         flag[b] = outcome;
         scale[b] = 1.0 / sqrt(keep);
         if (d.is_measure) {
@@ -126,8 +138,8 @@ __global__ void k_b_decide(const double* __restrict__ partials, uint32_t nb, uin
         }
         if (p.x <= 0.0) continue;
         chosen = static_cast<int>(i);
-        chosen_p = p.x;
-        cum += p.x;
+        chosen_p = p.x;   // unnormalised: Tr(K rho K^dagger)
+        cum += p.x / tr;
         if (u < cum) break;
     }
     if (chosen < 0) {
@@ -217,7 +229,7 @@ void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t b
                        uint64_t per_shot, TrajScratch& s) {
     const uint64_t len = uint64_t{1} << n;
     const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
-    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials);
+    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials, d.forced);
     check_launch("traj_rdm1");
     k_b_decide<<<(batch + 127) / 128, 128, 0, ctx.stream>>>(s.partials, nb, batch, d, d_uniforms,
                                                              first, per_shot, s.mats, s.flag,
@@ -232,7 +244,7 @@ void launch_traj_measure(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t
                          uint64_t first, uint64_t per_shot, int reset, TrajScratch& s) {
     const uint64_t len = uint64_t{1} << n;
     const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
-    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials);
+    k_b_rdm1<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, s.partials, nullptr);
     check_launch("traj_rdm1");
     k_b_decide<<<(batch + 127) / 128, 128, 0, ctx.stream>>>(s.partials, nb, batch, d, d_uniforms,
                                                              first, per_shot, s.mats, s.flag,

@@ -11,6 +11,7 @@
 // host synchronisation until its registers are read back.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "engine.hpp"
 #include "traj.cuh"
@@ -51,6 +52,215 @@ bool is_identity_scaled(const Kraus& m) {
     constexpr double tol = 1e-14;
     return std::abs(m[1]) < tol && std::abs(m[2]) < tol && std::abs(m[0] - cd{1, 0}) < tol &&
            std::abs(m[3] - cd{1, 0}) < tol;
+}
+
+bool use_fused(uint32_t n) {
+    if (n < kRegMinBits) return false;
+    const char* e = std::getenv("LQCS_TRAJ_FUSED");
+    return !(e && e[0] == '0');
+}
+
+// lambda_min(K^dagger K): for every state, Tr(K rho K^dagger) / Tr(rho) >= this bound.
+double min_eig_kdk(const Kraus& k) {
+    const double a = std::norm(k[0]) + std::norm(k[2]), d = std::norm(k[1]) + std::norm(k[3]);
+    const double b = std::abs(std::conj(k[0]) * k[1] + std::conj(k[2]) * k[3]);
+    return 0.5 * (a + d) - std::sqrt(0.25 * (a - d) * (a - d) + b * b);
+}
+
+GateDesc matrix_gate(uint32_t q, const Kraus& m) {
+    GateDesc g;
+    g.type = LQCS_GATE_UNITARY;
+    g.qubits = {q};
+    g.mat.assign(m.begin(), m.end());
+    return g;
+}
+
+struct FusedRun {
+    uint32_t n;
+    const std::vector<Item>& items;
+    const std::vector<std::vector<GateDesc>>& stretches;
+    const std::vector<Channel>& channels;
+    const std::vector<std::vector<Kraus>>& norm;        // unitary mixtures: normalised ops
+    const std::vector<const DeviceBuffer*>& ops_dev;     // raw operators on the device
+    const std::vector<std::vector<int>>& choice;         // unitary-mixture items: branch per shot
+    const std::vector<double>& u;
+    uint32_t K;
+    uint64_t shots;
+    uint32_t max_resident;
+};
+
+// Fused batches.  Every noise event whose branch is fixed before the run is a matrix in
+// the gate stream: a unitary-mixture branch (chosen from its uniform alone) and the first
+// operator K0 of a general channel when u < lambda_min(K0^dagger K0) - 1e-12, because then
+// u < Tr(K0 rho K0^dagger) / Tr(rho) for every state, so the reference's first-branch rule
+// picks K0 whatever the state.  K0 is applied without its 1/sqrt(p0): states stay
+// unnormalised until a state-dependent event, which takes probabilities relative to the
+// state's norm and renormalises.  A branch fixed for all states of the batch is one shared
+// gate; one that differs is a noise slot (per-state 2x2).  Only events whose branch depends
+// on the state (some uncertain general channel, Measure, Reset) cut the batch's gate stream;
+// between cuts the stream runs as register tile passes over the whole batch.
+void run_fused(const FusedRun& f, uint64_t* regs) {
+    const uint32_t n = f.n;
+    std::vector<double> lam(f.channels.size(), 0.0);
+    for (size_t c = 0; c < f.channels.size(); ++c) lam[c] = min_eig_kdk(f.channels[c][0]);
+    // batch work on its own stream; program uploads on another, so the host compiles the next
+    // segment while the device runs the current one
+    cudaStream_t cs = nullptr, us = nullptr;
+    cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
+    struct Streams {
+        cudaStream_t a = nullptr, b = nullptr;
+        ~Streams() {
+            if (a) cudaStreamDestroy(a);
+            if (b) cudaStreamDestroy(b);
+        }
+    } guard;
+    guard.a = cs;
+    cuda_check(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking), "cudaStreamCreate");
+    guard.b = us;
+
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const uint64_t state_bytes = uint64_t{16} << n;
+    const uint64_t fit = std::max<uint64_t>(1, static_cast<uint64_t>(free_b * 0.85) / state_bytes);
+    const uint32_t R = static_cast<uint32_t>(std::min<uint64_t>(
+        {f.shots, fit, f.max_resident ? f.max_resident : uint64_t{1024}}));
+    auto st = new_state(n, R, cs);
+    const LaunchCtx ctx = st->ctx;
+
+    DeviceBuffer d_u, part, mats, flag, scale, dregs;
+    d_u.ensure(sizeof(double) * std::max<size_t>(1, f.u.size()));
+    if (!f.u.empty())
+        cuda_check(cudaMemcpy(d_u.ptr, f.u.data(), sizeof(double) * f.u.size(), cudaMemcpyHostToDevice),
+                   "H2D uniforms");
+    part.ensure(sizeof(double) * R * 4 * kTrajMaxBlocks);
+    mats.ensure(sizeof(double2) * R * 4);
+    flag.ensure(sizeof(int) * R);
+    scale.ensure(sizeof(double) * R);
+    dregs.ensure(sizeof(uint64_t) * R);
+    TrajScratch scr{part.as<double>(), mats.as<double2>(), flag.as<int>(), scale.as<double>(),
+                    dregs.as<uint64_t>()};
+    const Kraus ident{cd{1, 0}, cd{0, 0}, cd{0, 0}, cd{1, 0}};
+
+    for (uint64_t first = 0; first < f.shots; first += R) {
+        const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(R, f.shots - first));
+        launch_set_basis(ctx, st->d(), n, nb, 0);
+        cuda_check(cudaMemsetAsync(dregs.ptr, 0, sizeof(uint64_t) * nb, cs), "memset");
+        std::vector<Program> keep;          // alive until the batch is done
+        std::vector<DeviceBuffer> bufs;
+        std::vector<GateDesc> seg;
+        std::vector<std::vector<Kraus>> slots(nb);
+        auto upload = [&](const void* src, size_t bytes) {
+            DeviceBuffer b;
+            b.ensure(bytes);
+            cuda_check(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, us), "H2D batch data");
+            cuda_check(cudaStreamSynchronize(us), "H2D batch data");
+            bufs.push_back(std::move(b));
+            return bufs.back().ptr;
+        };
+        auto flush = [&]() {
+            if (seg.empty()) return;
+            Program p;
+            if (compile_slots(seg, n, slots, us, p)) {
+                p.launch(ctx, st->d(), n, nb);
+                keep.push_back(std::move(p));
+            } else {
+                // gate by gate: shared gates as programs, noise slots as per-state 2x2 tables
+                FusionConfig none;
+                none.fuse = false;
+                for (const GateDesc& g : seg) {
+                    if (!g.slot) {
+                        keep.push_back(compile({g}, n, none, us));
+                        keep.back().launch(ctx, st->d(), n, nb);
+                        continue;
+                    }
+                    std::vector<double2> tab(4 * static_cast<size_t>(nb));
+                    std::vector<int> idx(nb);
+                    for (uint32_t b = 0; b < nb; ++b) {
+                        for (int e = 0; e < 4; ++e) {
+                            const cd z = slots[b][g.slot_id][e];
+                            tab[4 * b + e] = make_double2(z.real(), z.imag());
+                        }
+                        idx[b] = static_cast<int>(b);
+                    }
+                    const void* dt = upload(tab.data(), sizeof(double2) * tab.size());
+                    const void* di = upload(idx.data(), sizeof(int) * idx.size());
+                    launch_traj_table(ctx, st->d(), n, nb, g.qubits[0],
+                                      static_cast<const double2*>(dt), static_cast<const int*>(di));
+                }
+            }
+            seg.clear();
+            for (auto& s : slots) s.clear();
+        };
+        for (size_t i = 0; i < f.items.size(); ++i) {
+            const Item& it = f.items[i];
+            switch (it.kind) {
+                case kUnitary:
+                    seg.insert(seg.end(), f.stretches[it.prog].begin(), f.stretches[it.prog].end());
+                    break;
+                case kKrausTable: {
+                    const std::vector<int>& ch = f.choice[i];
+                    const int c0 = ch[first];
+                    bool any = false, same = true;
+                    for (uint32_t b = 0; b < nb; ++b) {
+                        any |= ch[first + b] >= 0;
+                        same &= ch[first + b] == c0;
+                    }
+                    if (!any) break;
+                    if (same) {
+                        seg.push_back(matrix_gate(it.q, f.norm[it.channel][c0]));
+                        break;
+                    }
+                    GateDesc g = matrix_gate(it.q, ident);
+                    g.slot = true;
+                    g.slot_id = static_cast<uint32_t>(slots[0].size());
+                    for (uint32_t b = 0; b < nb; ++b) {
+                        const int c = ch[first + b];
+                        slots[b].push_back(c < 0 ? ident : f.norm[it.channel][c]);
+                    }
+                    seg.push_back(std::move(g));
+                    break;
+                }
+                case kKrausGeneral: {
+                    const double bound = lam[it.channel] - 1e-12;
+                    std::vector<int> forced(nb);
+                    bool all = true;
+                    for (uint32_t b = 0; b < nb; ++b) {
+                        forced[b] = f.u[(first + b) * f.K + it.uidx] < bound ? 0 : -1;
+                        all &= forced[b] == 0;
+                    }
+                    if (all) {
+                        seg.push_back(matrix_gate(it.q, f.channels[it.channel][0]));
+                        break;
+                    }
+                    flush();
+                    TrajDecide d{};
+                    d.mode = 0;
+                    d.uniform_index = it.uidx;
+                    d.n_ops = static_cast<uint32_t>(f.channels[it.channel].size());
+                    d.ops = f.ops_dev[it.channel]->as<double2>();
+                    d.forced = static_cast<const int*>(upload(forced.data(), sizeof(int) * nb));
+                    launch_traj_kraus(ctx, st->d(), n, nb, it.q, d, d_u.as<double>(), first, f.K, scr);
+                    break;
+                }
+                case kMeasure:
+                case kReset: {
+                    flush();
+                    TrajDecide d{};
+                    d.mode = 1;
+                    d.is_measure = it.kind == kMeasure ? 1 : 0;
+                    d.clbit = it.clbit;
+                    d.uniform_index = it.uidx;
+                    launch_traj_measure(ctx, st->d(), n, nb, it.q, d, d_u.as<double>(), first, f.K,
+                                        it.kind == kReset ? 1 : 0, scr);
+                    break;
+                }
+            }
+        }
+        flush();
+        cuda_check(cudaMemcpyAsync(regs + first, dregs.ptr, sizeof(uint64_t) * nb,
+                                   cudaMemcpyDeviceToHost, cs), "D2H registers");
+        cuda_check(cudaStreamSynchronize(cs), "trajectory batch");
+    }
 }
 
 }  // namespace
@@ -148,6 +358,7 @@ void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64
     }
     // per table item: branch per shot (-1 = identity, nothing to apply)
     std::vector<DeviceBuffer> choice(items.size());
+    std::vector<std::vector<int>> choice_host(items.size());
     for (size_t i = 0; i < items.size(); ++i) {
         Item& it = items[i];
         if (it.kind != kKrausGeneral || !cdev[it.channel].table) continue;
@@ -169,6 +380,20 @@ void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64
         choice[i].ensure(sizeof(int) * shots);
         cuda_check(cudaMemcpy(choice[i].ptr, ch.data(), sizeof(int) * shots, cudaMemcpyHostToDevice),
                    "H2D branch table");
+        choice_host[i] = std::move(ch);
+    }
+
+    if (fc_in.fuse && use_fused(n)) {
+        std::vector<std::vector<Kraus>> norm(channels.size());
+        std::vector<const DeviceBuffer*> ops_dev(channels.size());
+        for (size_t c = 0; c < channels.size(); ++c) {
+            norm[c] = cdev[c].norm;
+            ops_dev[c] = &cdev[c].ops;
+        }
+        const FusedRun fr{n, items, stretches, channels, norm, ops_dev, choice_host, u, K, shots,
+                          max_resident};
+        run_fused(fr, regs);
+        return;
     }
 
     // ---- resident batch

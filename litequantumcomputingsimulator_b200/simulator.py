@@ -189,7 +189,8 @@ class CompiledCircuit:
                 name += f"<{r.n_targets}>"
             out.append({"kernel": name, "kind": r.kind, "width": r.n_targets, "gates": r.n_gates,
                         "min_target": r.min_target, "max_target": r.max_target,
-                        "controls": r.n_controls, "ms": r.device_ms, "alg_bytes": r.alg_bytes})
+                        "controls": r.n_controls, "ms": r.device_ms, "alg_bytes": r.alg_bytes,
+                        "alg_flops": r.alg_flops})
         return out
 
 

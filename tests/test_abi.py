@@ -59,7 +59,7 @@ int main(void) {
   P(lqcs_parametric_circuit, n_insts); P(lqcs_parametric_circuit, param_inst);
   printf("lqcs_hamiltonian %zu\\n", sizeof(lqcs_hamiltonian));
   printf("lqcs_op_profile %zu\\n", sizeof(lqcs_op_profile));
-  P(lqcs_op_profile, device_ms); P(lqcs_op_profile, alg_bytes);
+  P(lqcs_op_profile, device_ms); P(lqcs_op_profile, alg_bytes); P(lqcs_op_profile, alg_flops);
   return 0;
 }
 """)
@@ -88,6 +88,7 @@ def test_struct_layouts_match_header(tmp_path):
     assert c["lqcs_op_profile"] == C.sizeof(N.OpProfile)
     assert c["lqcs_op_profile.device_ms"] == N.OpProfile.device_ms.offset
     assert c["lqcs_op_profile.alg_bytes"] == N.OpProfile.alg_bytes.offset
+    assert c["lqcs_op_profile.alg_flops"] == N.OpProfile.alg_flops.offset
 
 
 def test_null_arguments_are_rejected_with_messages():

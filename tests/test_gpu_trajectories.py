@@ -66,3 +66,37 @@ def test_config3_cross_check_tvd(ref):
         boot.append(0.5 * np.abs(np.bincount(draw, minlength=1 << n) / shots - exact).sum())
     assert tvd <= np.quantile(boot, 0.999)
     assert tvd >= np.quantile(boot, 0.001)
+
+
+# ---- fused batches (n >= 9): fixed-branch noise fused into register tile passes
+
+
+@pytest.mark.parametrize("resident", [5, 64])
+def test_fused_explicit_kraus_counts_identical(ref, resident):
+    """Heavy noise: many uncertain amplitude-damping events (cuts) and differing Pauli
+    branches per state (noise slots); counts equal the reference's per-shot semantics."""
+    qc = W.brickwork(10, 6, seed=8, measure=True, noise=(0.05, 0.1, 0.2))
+    want = counts_of(ref.trajectories(qc, 128, 33))
+    got = counts_of(lq.StatevectorSimulator(seed=33, max_resident=resident).run_registers(qc, 128))
+    assert got == want
+
+
+def test_fused_noise_model_counts_identical(ref):
+    noise = lq.NoiseModel()
+    noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.05))
+    noise.add_all_qubit_channel(lq.KrausChannel.amplitude_damping(0.1))
+    qc = W.brickwork(9, 4, seed=12, measure=True)
+    want = ref.run(qc, 96, 5, noise=noise)
+    got = counts_of(lq.StatevectorSimulator(seed=5, noise=noise, max_resident=32)
+                    .run_registers(qc, 96))
+    assert got == want
+
+
+def test_fused_matches_unfused_at_config3_rates(monkeypatch):
+    """Config-3 noise rates at 14 qubits: the fused driver and the gate-by-gate driver give
+    the same registers for the same seed."""
+    qc = W.brickwork(14, 8, seed=21, measure=True, noise=(1e-3, 1e-2, 1e-3))
+    fused = lq.StatevectorSimulator(seed=7, max_resident=32).run_registers(qc, 96)
+    monkeypatch.setenv("LQCS_TRAJ_FUSED", "0")
+    plain = lq.StatevectorSimulator(seed=7, max_resident=32).run_registers(qc, 96)
+    assert np.array_equal(fused, plain)
