@@ -17,7 +17,8 @@ struct TrajDecide {
     uint32_t n_ops;           // mode 0: Kraus operators (2x2 each, device memory)
     const double2* ops;
     const int* forced;        // mode 0, optional (device, per state): branch >= 0 known in
-                              // advance -> K_branch applied unnormalised, no reduction
+                              // advance -> the state is left alone here (no reduction, nothing
+                              // applied); the caller applies that branch elsewhere
 };
 
 // Device scratch for a resident batch of R trajectories.
@@ -39,6 +40,13 @@ void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t b
 void launch_traj_measure(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
                          uint32_t q, const TrajDecide& d, const double* d_uniforms,
                          uint64_t first, uint64_t per_shot, int reset, TrajScratch& s);
+// Terminal measurement of qubit q without collapsing: state b's amplitudes consistent with
+// its earlier terminal outcomes (bits `fixed` equal to vals[b]) give p1 relative to their
+// total; the outcome is recorded in vals[b] (bit q) and in the classical register.
+void launch_traj_tail_measure(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                              uint32_t batch, uint32_t q, const BitList& fixed, uint64_t* vals,
+                              uint32_t clbit, uint32_t uniform_index, const double* d_uniforms,
+                              uint64_t first, uint64_t per_shot, TrajScratch& s);
 // Per-state choice into a table of normalised 2x2 operators (choice < 0: no-op).
 void launch_traj_table(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
                        const double2* d_mats, const int* d_choice);

@@ -88,8 +88,8 @@ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -
 // mode 0 (Kraus): probabilities p_i = Tr(K_i rho K_i^dagger) / t, first i with
 //                 u < cumulative p (p <= 0 skipped, last non-zero branch as fallback),
 //                 mats[b] = K_i / sqrt(p_i t), flag[b] = 1 (0 only when every probability is
-//                 zero: nothing is applied).  A forced branch (forced[b] >= 0) is applied as
-//                 K_i, without reduction or normalisation.
+//                 zero: nothing is applied).  A state with a forced branch (forced[b] >= 0)
+//                 is left alone.
 // mode 1 (measure/reset): p1 = rho11 / t, outcome = u < p1, scale 1/sqrt(rho_oo); the clbit
 //                 of the register is set or cleared (measure only).
 __global__ void k_b_decide(const double* __restrict__ partials, uint32_t nb, uint32_t batch,
@@ -99,9 +99,7 @@ __global__ void k_b_decide(const double* __restrict__ partials, uint32_t nb, uin
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= batch) return;
     if (d.mode == 0 && d.forced && d.forced[b] >= 0) {
-        const double2* k = d.ops + 4 * d.forced[b];
-        for (int e = 0; e < 4; ++e) mats[4 * b + e] = k[e];
-        flag[b] = 1;
+        flag[b] = 0;   // branch known in advance: applied by the caller
         return;
     }
     double r[4] = {0, 0, 0, 0};
@@ -222,6 +220,46 @@ __global__ void __launch_bounds__(kThreads) k_b_apply_table(double2* __restrict_
     }
 }
 
+// Sum of |a|^2 over the amplitudes of state b whose bits at `fixed` equal vals[b], split by
+// bit q (values 0 and 1 of the partials row; 2 and 3 stay zero).
+__global__ void __launch_bounds__(kThreads) k_b_tail_sum(const double2* __restrict__ st,
+                                                         uint64_t len, uint32_t q, BitList fixed,
+                                                         const uint64_t* __restrict__ vals,
+                                                         double* __restrict__ partials) {
+    const double2* s = st + static_cast<uint64_t>(blockIdx.y) * len;
+    const uint64_t val = vals[blockIdx.y];
+    const uint64_t count = len >> fixed.n;
+    double v[4] = {0, 0, 0, 0};
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += stride) {
+        const uint64_t x = expand_bits(i, fixed) | val;
+        const double2 a = __ldg(s + x);
+        v[(x >> q) & 1] += a.x * a.x + a.y * a.y;
+    }
+    block_sum<4>(v, partials + static_cast<uint64_t>(blockIdx.y) * 4 * gridDim.x + blockIdx.x,
+                 gridDim.x);
+}
+
+__global__ void k_b_tail_decide(const double* __restrict__ partials, uint32_t nb, uint32_t batch,
+                                const double* __restrict__ uniforms, uint64_t first,
+                                uint64_t per_shot, uint32_t uidx, uint32_t q, uint32_t clbit,
+                                uint64_t* __restrict__ vals, uint64_t* __restrict__ regs) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    double r0 = 0.0, r1 = 0.0;
+    const double* row = partials + static_cast<uint64_t>(b) * 4 * nb;
+    for (uint32_t j = 0; j < nb; ++j) {
+        r0 += row[j];
+        r1 += row[nb + j];
+    }
+    const double u = uniforms[(first + b) * per_shot + uidx];
+    const int outcome = u < r1 / (r0 + r1) ? 1 : 0;
+    if (outcome) vals[b] |= uint64_t{1} << q;
+    const uint64_t bit = uint64_t{1} << clbit;
+    regs[b] = outcome ? (regs[b] | bit) : (regs[b] & ~bit);
+}
+
 }  // namespace
 
 void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
@@ -260,6 +298,24 @@ void launch_traj_table(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t b
     const uint32_t nb = blocks_per_state(ctx, len >> 1, batch);
     k_b_apply_table<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, d_mats, d_choice);
     check_launch("traj_table");
+}
+
+}  // namespace lqcs_b200
+
+namespace lqcs_b200 {
+
+void launch_traj_tail_measure(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                              uint32_t batch, uint32_t q, const BitList& fixed, uint64_t* vals,
+                              uint32_t clbit, uint32_t uniform_index, const double* d_uniforms,
+                              uint64_t first, uint64_t per_shot, TrajScratch& s) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t nb = blocks_per_state(ctx, len >> fixed.n, batch);
+    k_b_tail_sum<<<dim3(nb, batch), kThreads, 0, ctx.stream>>>(st, len, q, fixed, vals, s.partials);
+    check_launch("traj_tail_sum");
+    k_b_tail_decide<<<(batch + 127) / 128, 128, 0, ctx.stream>>>(s.partials, nb, batch, d_uniforms,
+                                                                  first, per_shot, uniform_index, q,
+                                                                  clbit, vals, s.regs);
+    check_launch("traj_tail_decide");
 }
 
 }  // namespace lqcs_b200

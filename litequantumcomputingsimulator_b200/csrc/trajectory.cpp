@@ -140,11 +140,25 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
     TrajScratch scr{part.as<double>(), mats.as<double2>(), flag.as<int>(), scale.as<double>(),
                     dregs.as<uint64_t>()};
     const Kraus ident{cd{1, 0}, cd{0, 0}, cd{0, 0}, cd{1, 0}};
+    // Terminal measurements (nothing but Measures of distinct qubits up to the end) need no
+    // collapse: each outcome follows from the amplitudes consistent with the earlier ones.
+    size_t tail = f.items.size();
+    {
+        std::vector<char> seen(n, 0);
+        while (tail > 0 && f.items[tail - 1].kind == kMeasure && !seen[f.items[tail - 1].q]) {
+            seen[f.items[tail - 1].q] = 1;
+            --tail;
+        }
+    }
+    DeviceBuffer d_vals;
+    d_vals.ensure(sizeof(uint64_t) * R);
 
     for (uint64_t first = 0; first < f.shots; first += R) {
         const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(R, f.shots - first));
         launch_set_basis(ctx, st->d(), n, nb, 0);
         cuda_check(cudaMemsetAsync(dregs.ptr, 0, sizeof(uint64_t) * nb, cs), "memset");
+        cuda_check(cudaMemsetAsync(d_vals.ptr, 0, sizeof(uint64_t) * nb, cs), "memset");
+        BitList tail_fixed{};
         std::vector<Program> keep;          // alive until the batch is done
         std::vector<DeviceBuffer> bufs;
         std::vector<GateDesc> seg;
@@ -240,9 +254,27 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
                     d.ops = f.ops_dev[it.channel]->as<double2>();
                     d.forced = static_cast<const int*>(upload(forced.data(), sizeof(int) * nb));
                     launch_traj_kraus(ctx, st->d(), n, nb, it.q, d, d_u.as<double>(), first, f.K, scr);
+                    // the states whose branch was known take K0 as the first gate of the next
+                    // segment (identity for the states decided here)
+                    GateDesc g = matrix_gate(it.q, ident);
+                    g.slot = true;
+                    g.slot_id = static_cast<uint32_t>(slots[0].size());
+                    for (uint32_t b = 0; b < nb; ++b)
+                        slots[b].push_back(forced[b] == 0 ? f.channels[it.channel][0] : ident);
+                    seg.push_back(std::move(g));
                     break;
                 }
                 case kMeasure:
+                    if (i >= tail) {   // terminal: Born rule on the consistent subspace
+                        flush();
+                        launch_traj_tail_measure(ctx, st->d(), n, nb, it.q, tail_fixed,
+                                                 d_vals.as<uint64_t>(), it.clbit, it.uidx,
+                                                 d_u.as<double>(), first, f.K, scr);
+                        tail_fixed.pos[tail_fixed.n++] = it.q;
+                        std::sort(tail_fixed.pos, tail_fixed.pos + tail_fixed.n);
+                        break;
+                    }
+                    [[fallthrough]];
                 case kReset: {
                     flush();
                     TrajDecide d{};

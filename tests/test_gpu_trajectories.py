@@ -100,3 +100,17 @@ def test_fused_matches_unfused_at_config3_rates(monkeypatch):
     monkeypatch.setenv("LQCS_TRAJ_FUSED", "0")
     plain = lq.StatevectorSimulator(seed=7, max_resident=32).run_registers(qc, 96)
     assert np.array_equal(fused, plain)
+
+
+def test_fused_terminal_measures_any_order(ref):
+    """Terminal measurements of a qubit subset in arbitrary order, into permuted clbits, after
+    a mid-circuit measurement and reset: counts equal the reference's."""
+    qc = W.brickwork(11, 3, seed=40, noise=(0.02, 0.05, 0.3))
+    full = lq.QuantumCircuit(11, 6)
+    full.compose(qc)
+    full.measure(4, 5).reset(4).h(4).cx(4, 9)
+    for q, c in ((7, 0), (2, 3), (9, 1), (0, 4), (10, 2)):
+        full.measure(q, c)
+    want = counts_of(ref.trajectories(full, 160, 71))
+    got = counts_of(lq.StatevectorSimulator(seed=71, max_resident=40).run_registers(full, 160))
+    assert got == want
