@@ -515,6 +515,37 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     except Exception as ex:  # noqa: BLE001
         out["trajectories_error"] = str(ex)
 
+    # wide fused blocks: 28-qubit brickwork depth 20 fused greedily to 6-qubit blocks, on the
+    # FP64 tensor path (mma.sync.m8n8k4.f64) and on the FFMA kernel
+    try:
+        wq = W.brickwork(28, 20, seed=55)
+        wsv = lq.Statevector(28)
+        wprog = lq.simulator.CompiledCircuit(wq, True, 6, 1)
+        res = {}
+        for name, flag in (("dmma", "1"), ("ffma", "0")):
+            os.environ["LQCS_DENSE_MMA"] = flag
+            try:
+                wprog.apply(wsv)
+                torch.cuda.synchronize()
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
+                wprog.apply(wsv)
+                e.record()
+                torch.cuda.synchronize()
+                res[name] = s.elapsed_time(e)
+            finally:
+                os.environ.pop("LQCS_DENSE_MMA", None)
+        prof = wprog.profile(wsv)
+        k6 = [r for r in prof if r["kernel"] == "k_dense<6>"]
+        out["width6_28q_ms"] = {k: round(v, 2) for k, v in res.items()}
+        out["width6_28q_dmma_speedup"] = res["ffma"] / res["dmma"]
+        if k6:
+            out["width6_dmma_k6_tflops"] = (sum(r["alg_flops"] for r in k6) /
+                                            (sum(r["ms"] for r in k6) / 1e3) / 1e12)
+        del wsv
+    except Exception as ex:  # noqa: BLE001
+        out["width6_error"] = str(ex)
+
     # learned fusion cost model: trained on the engine's own per-operation timings of
     # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the
     # greedy plan of a held-out 32-qubit circuit (64 GiB state) are timed on the device

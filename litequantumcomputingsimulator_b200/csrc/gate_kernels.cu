@@ -298,6 +298,10 @@ static void dense_impl(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t b
 void launch_dense(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
                   const uint32_t* targets, uint32_t k, uint64_t cmask,
                   const double2* d_mat) {
+    if (dense_mma_enabled(k)) {   // wide blocks on the FP64 tensor path
+        launch_dense_mma(ctx, st, n, batch, targets, k, cmask, d_mat);
+        return;
+    }
     switch (k) {
         case 1: dense_impl<1>(ctx, st, n, batch, targets, cmask, d_mat); break;
         case 2: dense_impl<2>(ctx, st, n, batch, targets, cmask, d_mat); break;

@@ -44,6 +44,11 @@ void launch_phase(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
 void launch_dense(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
                   const uint32_t* targets, uint32_t k, uint64_t cmask,
                   const double2* d_mat);
+// The same on the FP64 tensor path (mma.sync.m8n8k4.f64, dense_mma_kernels.cu), k = 4..6;
+// launch_dense routes there where dense_mma_enabled(k) (LQCS_DENSE_MMA overrides).
+bool dense_mma_enabled(uint32_t k);
+void launch_dense_mma(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
+                      const uint32_t* targets, uint32_t k, uint64_t cmask, const double2* d_mat);
 
 // Diagonal k-qubit operator: amp *= diag[local index] (local bit j <-> targets[j]),
 // on the subspace where every control bit is 1.  Device memory diag of 2^k entries.

@@ -316,3 +316,18 @@ def test_errors_match_reference_types():
         _ = sv[4]
     with pytest.raises(ValueError, match="length must equal"):
         sv.expectation_value("ZZZ")
+
+
+@pytest.mark.parametrize("width", [4, 5, 6])
+@pytest.mark.parametrize("mma", ["1", "0"])
+def test_wide_blocks_dmma_and_ffma(port, monkeypatch, width, mma):
+    """Greedy 4..6-qubit blocks (controls included) on the FP64 tensor path
+    (mma.sync.m8n8k4.f64) and on the FFMA kernel agree with the oracle."""
+    monkeypatch.setenv("LQCS_DENSE_MMA", mma)
+    n = 14
+    init = W.gaussian_state(n, seed=width)
+    qc = random_circuit(n, 80, seed=100 + width, max_controls=3, max_unitary=4)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    sv = lq.Statevector.from_numpy(init)
+    sv.apply(qc, fuse_gates=True, max_fusion_width=width, fusion_mode=1)
+    assert np.max(np.abs(sv.to_numpy() - want)) < 1e-12
