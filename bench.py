@@ -546,6 +546,23 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     except Exception as ex:  # noqa: BLE001
         out["width6_error"] = str(ex)
 
+    # autotuner: every candidate plan of a 28-qubit brickwork (depth 40) timed on the device;
+    # the chosen plan against the default one
+    try:
+        aq = W.brickwork(28, 40, seed=66)
+        t0 = time.perf_counter()
+        tune = lq.simulator.autotune(aq)
+        out["autotune_28q_s"] = time.perf_counter() - t0
+        out["autotune_28q"] = [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()}
+                               for r in tune]
+        chosen = [r for r in tune if r["chosen"]]
+        default = [r for r in tune if r["planner"] == "register tile passes" and
+                   r["tile_bits"] == 12 and r["inner"] == 2]
+        if chosen and default:
+            out["autotune_28q_gain_vs_default"] = default[0]["ms"] / chosen[0]["ms"]
+    except Exception as ex:  # noqa: BLE001
+        out["autotune_error"] = str(ex)
+
     # learned fusion cost model: trained on the engine's own per-operation timings of
     # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the
     # greedy plan of a held-out 32-qubit circuit (64 GiB state) are timed on the device

@@ -97,7 +97,8 @@ typedef struct lqcs_kraus_channel {
  * Engine knobs (no counterpart in Options; zero means "engine default"):
  *   max_fusion_width : widest dense block the fusion pass may emit (1..6)
  *   fusion_mode      : 0 = default planner, 1 = greedy, 2 = learned cost model,
- *                      3 = gate-by-gate (no fusion even if fuse_gates)
+ *                      3 = gate-by-gate (no fusion even if fuse_gates), 4 = tile passes,
+ *                      5 = autotuned (lqcs_autotune's measured choice)
  *   max_resident     : most noise trajectories held on the device at once. */
 typedef struct lqcs_sim_options {
     uint64_t seed;
@@ -343,6 +344,28 @@ int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonia
 int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
                      int32_t max_fusion_width, int32_t fusion_mode, uint64_t cap,
                      uint32_t* block_width, uint32_t* block_gates, uint64_t* n_blocks);
+
+/* ------------------------------------------------------------------ autotuner
+ * Engine extension (no counterpart in the reference, whose fusion pass has no knobs):
+ * times every candidate fusion plan of the circuit — register tile passes of tile sizes
+ * 2^11..2^13 and inner widths 2..3, shared-memory tile passes, greedy dense blocks of width
+ * 4..6 — once each (after one untimed application) on a scratch n-qubit state allocated for
+ * the call, and remembers the fastest for this circuit; fusion_mode 5 then compiles with it
+ * (tuning on first use).  Needs 16 * 2^n bytes free for the scratch state; without them
+ * *n_out is 0 and fusion_mode 5 uses the default plan. */
+typedef struct lqcs_tune_entry {
+    int32_t planner;        /* 0 register tile passes, 1 shared-memory tile passes, 2 greedy */
+    uint32_t tile_bits;     /* tile passes: 2^tile_bits amplitudes per tile */
+    uint32_t tile_low;      /* tile passes: qubits 0..tile_low-1 always in the tile */
+    uint32_t inner;         /* tile passes: widest block fused inside a pass */
+    uint32_t width;         /* greedy: widest block */
+    uint32_t chosen;        /* 1 for the fastest candidate */
+    uint64_t n_ops;         /* device operations (launches) of one application */
+    double device_ms;       /* one application, CUDA events */
+} lqcs_tune_entry;
+
+int lqcs_autotune(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                  uint64_t cap, lqcs_tune_entry* out, uint64_t* n_out);
 
 /* ------------------------------------------------------------------ cost model
  * A 3-layer, 64-wide FP32 MLP predicting the device time of one device operation from

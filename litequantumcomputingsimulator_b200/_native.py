@@ -84,6 +84,19 @@ class HamiltonianC(C.Structure):
     ]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [
+        ("planner", C.c_int32),
+        ("tile_bits", C.c_uint32),
+        ("tile_low", C.c_uint32),
+        ("inner", C.c_uint32),
+        ("width", C.c_uint32),
+        ("chosen", C.c_uint32),
+        ("n_ops", C.c_uint64),
+        ("device_ms", C.c_double),
+    ]
+
+
 class OpProfile(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32),
@@ -149,6 +162,8 @@ SIGNATURES = {
     "lqcs_fusion_plan": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32, C.c_int32,
                                    C.c_uint64, C.c_void_p, C.c_void_p, _P(C.c_uint64)]),
     "lqcs_rng_uniforms": (C.c_int, [C.c_uint64, C.c_uint64, C.c_void_p]),
+    "lqcs_autotune": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_uint64,
+                                _P(TuneEntry), _P(C.c_uint64)]),
     "lqcs_costmodel_features": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_uint32, C.c_uint32, C.c_void_p]),
     "lqcs_costmodel_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_float,

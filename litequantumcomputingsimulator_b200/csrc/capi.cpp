@@ -513,4 +513,27 @@ int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t 
     });
 }
 
+int lqcs_autotune(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                  uint64_t cap, lqcs_tune_entry* out, uint64_t* n_out) {
+    return guarded([&] {
+        need(n_out, "n_out");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        size_t best = 0;
+        const auto t = lqcs_b200::autotune(gates, n_qubits, &best);
+        *n_out = t.size();
+        for (size_t i = 0; i < t.size() && i < cap && out; ++i) {
+            lqcs_tune_entry& e = out[i];
+            e = lqcs_tune_entry{};
+            e.planner = t[i].cand.planner;
+            e.tile_bits = t[i].cand.planner == 2 ? 0 : t[i].cand.cfg.m;
+            e.tile_low = t[i].cand.planner == 2 ? 0 : t[i].cand.cfg.L;
+            e.inner = t[i].cand.planner == 2 ? 0 : t[i].cand.cfg.inner;
+            e.width = t[i].cand.width;
+            e.chosen = i == best ? 1u : 0u;
+            e.n_ops = t[i].n_ops;
+            e.device_ms = t[i].ms;
+        }
+    });
+}
+
 }  // extern "C"

@@ -366,9 +366,146 @@ bool compile_slots(const std::vector<GateDesc>& gates, uint32_t n,
     return true;
 }
 
+// ------------------------------------------------------------------ autotuner
+
+static std::vector<TuneCandidate> tune_candidates(uint32_t n) {
+    std::vector<TuneCandidate> c;
+    if (n >= kRegMinBits) {
+        const uint32_t shapes[][3] = {{12, 5, 2}, {12, 5, 3}, {11, 5, 2}, {13, 5, 2}};
+        for (const auto& s : shapes) {
+            TuneCandidate t;
+            t.cfg.m = std::min<uint32_t>(s[0], n);
+            t.cfg.L = std::min<uint32_t>(s[1], t.cfg.m);
+            t.cfg.inner = s[2];
+            bool dup = false;
+            for (const TuneCandidate& o : c)
+                dup |= o.planner == 0 && o.cfg.m == t.cfg.m && o.cfg.inner == t.cfg.inner;
+            if (!dup) c.push_back(t);
+        }
+        TuneCandidate smem;
+        smem.planner = 1;
+        smem.cfg.m = std::min<uint32_t>(12, n);
+        smem.cfg.reg = false;
+        c.push_back(smem);
+    }
+    for (uint32_t w = 2; w <= kMaxDense && w <= n; ++w) {
+        if (n >= kRegMinBits && w < 4) continue;   // narrow greedy blocks never beat tile passes
+        TuneCandidate t;
+        t.planner = 2;
+        t.width = w;
+        c.push_back(t);
+    }
+    return c;
+}
+
+static Program compile_candidate(const std::vector<GateDesc>& gates, uint32_t n,
+                                 const TuneCandidate& c, cudaStream_t stream) {
+    std::vector<DevOp> ops;
+    if (c.planner == 2) {
+        Program p;
+        p.build(dense_ops(gates, n, c.width), stream);
+        return p;
+    }
+    Program p = assemble_tiles(gates, n, c.cfg, ops);
+    p.build(std::move(ops), stream);
+    return p;
+}
+
+// FNV-1a over the gate list: the cache key of a tuned circuit.
+static uint64_t circuit_key(const std::vector<GateDesc>& gates, uint32_t n) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t len) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < len; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    mix(&n, sizeof n);
+    for (const GateDesc& g : gates) {
+        mix(&g.type, sizeof g.type);
+        mix(&g.n_controls, sizeof g.n_controls);
+        mix(g.qubits.data(), g.qubits.size() * sizeof(uint32_t));
+        mix(g.params.data(), g.params.size() * sizeof(double));
+        mix(g.mat.data(), g.mat.size() * sizeof(cd));
+        mix(g.perm.data(), g.perm.size() * sizeof(uint64_t));
+        mix(g.pauli.data(), g.pauli.size());
+    }
+    return h;
+}
+
+static std::mutex g_tune_mu;
+static std::map<uint64_t, TuneCandidate> g_tuned;
+
+std::vector<TuneTiming> autotune(const std::vector<GateDesc>& gates, uint32_t n, size_t* best) {
+    std::vector<TuneTiming> out;
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const double need = 16.0 * std::ldexp(1.0, static_cast<int>(n)) * 1.1 + (256u << 20);
+    if (need > static_cast<double>(free_b)) return out;
+    cudaStream_t s = nullptr;
+    cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    struct Guard {
+        cudaStream_t s;
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~Guard() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+            cudaStreamDestroy(s);
+        }
+    } guard{s};
+    cuda_check(cudaEventCreate(&guard.a), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&guard.b), "cudaEventCreate");
+    {
+        auto st = new_state(n, 1, s);
+        for (const TuneCandidate& c : tune_candidates(n)) {
+            Program p = compile_candidate(gates, n, c, s);
+            p.launch(st->ctx, st->d(), n, 1);   // untimed: first-launch set-up
+            cuda_check(cudaEventRecord(guard.a, s), "cudaEventRecord");
+            p.launch(st->ctx, st->d(), n, 1);
+            cuda_check(cudaEventRecord(guard.b, s), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(guard.b), "cudaEventSynchronize");
+            float ms = 0.0f;
+            cuda_check(cudaEventElapsedTime(&ms, guard.a, guard.b), "cudaEventElapsedTime");
+            out.push_back({c, p.ops.size(), ms});
+        }
+    }
+    size_t b = 0;
+    for (size_t i = 1; i < out.size(); ++i)
+        if (out[i].ms < out[b].ms) b = i;
+    if (best) *best = b;
+    if (!out.empty()) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[circuit_key(gates, n)] = out[b].cand;
+    }
+    return out;
+}
+
+// fusion_mode 5: the plan the autotuner measured fastest for this circuit (tuned now on a
+// cache miss); the default plan when no scratch state fits.
+static Program compile_autotuned(const std::vector<GateDesc>& gates, uint32_t n,
+                                 const FusionConfig& fc, cudaStream_t stream) {
+    const uint64_t key = circuit_key(gates, n);
+    std::optional<TuneCandidate> c;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        const auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) c = it->second;
+    }
+    if (!c) {
+        size_t best = 0;
+        const std::vector<TuneTiming> t = autotune(gates, n, &best);
+        if (!t.empty()) c = t[best].cand;
+    }
+    if (!c) {
+        FusionConfig d = fc;
+        d.mode = kFuseDefault;
+        return compile(gates, n, d, stream);
+    }
+    return compile_candidate(gates, n, *c, stream);
+}
+
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
                 cudaStream_t stream) {
     if (fc.fuse && fc.mode == kFuseLearned) return compile_learned(gates, n, fc, stream);
+    if (fc.fuse && fc.mode == kFuseAutotune) return compile_autotuned(gates, n, fc, stream);
     std::vector<DevOp> ops;
     if (use_tiles(n, fc)) {
         Program p = assemble_tiles(gates, n, default_tile_config(n), ops);

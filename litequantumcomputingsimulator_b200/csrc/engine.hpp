@@ -76,7 +76,27 @@ struct FusionConfig {
     uint32_t max_width = 0;   // 0 = engine default
     int mode = 0;             // 0 default, 1 greedy dense blocks, 2 learned, 3 none, 4 tile passes
 };
-enum FusionMode { kFuseDefault = 0, kFuseGreedy = 1, kFuseLearned = 2, kFuseNone = 3, kFuseTile = 4 };
+enum FusionMode {
+    kFuseDefault = 0, kFuseGreedy = 1, kFuseLearned = 2, kFuseNone = 3, kFuseTile = 4,
+    kFuseAutotune = 5
+};
+
+// One fusion plan the autotuner times: register or shared-memory tile passes of a shape, or
+// greedy dense blocks of a width.
+struct TuneCandidate {
+    int planner = 0;          // 0 register tile passes, 1 shared-memory tile passes, 2 greedy
+    TileConfig cfg;
+    uint32_t width = 0;
+};
+struct TuneTiming {
+    TuneCandidate cand;
+    uint64_t n_ops = 0;
+    double ms = 0.0;
+};
+// Times every candidate plan of `gates` once (after one untimed application) on a scratch
+// n-qubit state and remembers the fastest for this circuit; fusion_mode 5 compiles with it.
+// Empty when no scratch state fits in device memory (mode 5 then uses the default plan).
+std::vector<TuneTiming> autotune(const std::vector<GateDesc>& gates, uint32_t n, size_t* best);
 uint32_t default_fusion_width();
 
 // Compile a list of unitary gates to a Program (fused or gate by gate).

@@ -150,7 +150,8 @@ class Statevector:
 
 class CompiledCircuit:
     """A circuit fused and lowered once (``lqcs_program_create``); ``apply`` then costs only
-    kernel launches.  fusion_mode: 0 default, 1 greedy, 2 learned, 3 gate by gate."""
+    kernel launches.  fusion_mode: 0 default, 1 greedy, 2 learned, 3 gate by gate, 4 tile
+    passes, 5 autotuned (see autotune)."""
 
     def __init__(self, circuit: QuantumCircuit, fuse_gates: bool = True, max_fusion_width: int = 0,
                  fusion_mode: int = 0):
@@ -218,6 +219,27 @@ class Result:
         return f"<Result shots={self._shots} {{{body}}}>"
 
 
+_PLANNERS = {0: "register tile passes", 1: "shared-memory tile passes", 2: "greedy blocks"}
+
+
+def autotune(circuit) -> list:
+    """Time every candidate fusion plan of the circuit's unitary part on a scratch state
+    (lqcs_autotune) and remember the fastest: ``fusion_mode=5`` then uses it.  One dict per
+    candidate; empty when no scratch state fits in device memory."""
+    arr, n, _keep = circuit.c_instructions()
+    cap = 32
+    out = (N.TuneEntry * cap)()
+    cnt = C.c_uint64(0)
+    N.call("lqcs_autotune", circuit.num_qubits(), arr, n, cap, out, C.byref(cnt))
+    res = []
+    for i in range(min(cnt.value, cap)):
+        e = out[i]
+        res.append({"planner": _PLANNERS.get(e.planner, str(e.planner)), "tile_bits": e.tile_bits,
+                    "tile_low": e.tile_low, "inner": e.inner, "width": e.width,
+                    "chosen": bool(e.chosen), "n_ops": e.n_ops, "ms": e.device_ms})
+    return res
+
+
 def registers_to_counts(regs: np.ndarray, n_clbits: int) -> dict:
     """Count per-shot classical registers as the reference's MSB-left key strings."""
     vals, cnt = np.unique(regs, return_counts=True)
@@ -230,7 +252,8 @@ def registers_to_counts(regs: np.ndarray, n_clbits: int) -> dict:
 class StatevectorSimulator:
     """Drop-in for lqcs::StatevectorSimulator with the pylqcs keyword arguments
     (seed, fuse_gates, num_threads, noise).  Extra engine knobs: max_fusion_width,
-    fusion_mode (0 default, 1 greedy, 2 learned cost model, 3 gate by gate)."""
+    fusion_mode (0 default, 1 greedy, 2 learned cost model, 3 gate by gate, 4 tile passes,
+    5 autotuned)."""
 
     def __init__(self, seed: Optional[int] = None, fuse_gates: bool = True, num_threads: int = 0,
                  noise: Optional[NoiseModel] = None, *, max_fusion_width: int = 0,

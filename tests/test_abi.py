@@ -60,6 +60,8 @@ int main(void) {
   printf("lqcs_hamiltonian %zu\\n", sizeof(lqcs_hamiltonian));
   printf("lqcs_op_profile %zu\\n", sizeof(lqcs_op_profile));
   P(lqcs_op_profile, device_ms); P(lqcs_op_profile, alg_bytes); P(lqcs_op_profile, alg_flops);
+  printf("lqcs_tune_entry %zu\\n", sizeof(lqcs_tune_entry));
+  P(lqcs_tune_entry, n_ops); P(lqcs_tune_entry, device_ms);
   return 0;
 }
 """)
@@ -89,6 +91,9 @@ def test_struct_layouts_match_header(tmp_path):
     assert c["lqcs_op_profile.device_ms"] == N.OpProfile.device_ms.offset
     assert c["lqcs_op_profile.alg_bytes"] == N.OpProfile.alg_bytes.offset
     assert c["lqcs_op_profile.alg_flops"] == N.OpProfile.alg_flops.offset
+    assert c["lqcs_tune_entry"] == C.sizeof(N.TuneEntry)
+    assert c["lqcs_tune_entry.n_ops"] == N.TuneEntry.n_ops.offset
+    assert c["lqcs_tune_entry.device_ms"] == N.TuneEntry.device_ms.offset
 
 
 def test_null_arguments_are_rejected_with_messages():

@@ -169,3 +169,20 @@ def test_register_kernel_controls_phases_and_diagonals(port, tile_env):
     want = port.run_statevector(qc, fuse=False, state=init)
     assert 7 in kernel_kinds(qc)
     assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+
+
+def test_autotune_picks_a_timed_plan_and_mode5_uses_it(port):
+    """lqcs_autotune times every candidate plan; fusion_mode 5 compiles the fastest one and
+    gives the oracle's amplitudes."""
+    n = 16
+    qc = W.brickwork(n, 6, seed=19)
+    res = lq.simulator.autotune(qc)
+    assert len(res) >= 5 and sum(r["chosen"] for r in res) == 1
+    best = min(res, key=lambda r: r["ms"])
+    assert best["chosen"] and all(r["ms"] > 0 for r in res)
+    want = port.run_statevector(qc, fuse=False)
+    prog = lq.simulator.CompiledCircuit(qc, True, 0, 5)
+    sv = lq.Statevector(n)
+    prog.apply(sv)
+    assert np.max(np.abs(sv.to_numpy() - want)) < TOL
+    assert prog.n_ops == best["n_ops"]
