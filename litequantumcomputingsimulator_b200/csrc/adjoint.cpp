@@ -12,6 +12,10 @@
 // parameterised rotations read one (cos, sin) per state.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <mutex>
 
 #include "engine.hpp"
 
@@ -97,6 +101,205 @@ uint32_t default_resident(uint32_t n, uint64_t batch) {
 
 }  // namespace
 
+namespace {
+
+// Everything one (circuit, Hamiltonian, resident batch) needs on the device, kept between
+// calls: the fixed gates and their inverses, the two resident state batches, the Hamiltonian
+// terms and the per-set buffers, on a stream of its own.  A call only uploads the new
+// (cos, sin) tables, so the launch sequence of a batch of nb sets never changes: it is
+// captured once as a CUDA graph and replayed (LQCS_GRAPHS=0: launched directly).
+struct AdjointPlan {
+    uint64_t key = 0;
+    uint32_t n = 0, R = 0;
+    uint64_t np = 0;
+    std::vector<GateStep> steps;
+    std::vector<PauliTermDev> terms;
+    std::unique_ptr<lqcs_state> psi, lam;
+    DeviceBuffer d_terms, d_cs, d_csi, d_part, d_energy, d_grad;
+    cudaStream_t stream = nullptr;
+    std::map<uint32_t, std::pair<cudaGraphExec_t, uint64_t>> graphs;   // nb -> (graph, kernels)
+
+    AdjointPlan() = default;
+    AdjointPlan(const AdjointPlan&) = delete;
+    AdjointPlan& operator=(const AdjointPlan&) = delete;
+    ~AdjointPlan() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second.first);
+        psi.reset();
+        lam.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // The launch sequence of one batch of nb sets on this plan's stream.
+    void enqueue(uint32_t nb) const {
+        const LaunchCtx& ctx = psi->ctx;
+        const uint64_t len = uint64_t{1} << n;
+        launch_set_basis(ctx, psi->d(), n, nb, 0);
+        for (const GateStep& s : steps) {
+            if (s.param >= 0) {
+                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y,
+                                              d_cs.as<double2>() + static_cast<uint64_t>(s.param) * R);
+            } else {
+                s.fwd.launch(ctx, psi->d(), n, nb);
+            }
+        }
+        if (terms.empty()) {
+            cuda_check(cudaMemsetAsync(lam->d(), 0, sizeof(double2) * len * nb, ctx.stream), "memset");
+        } else {
+            launch_apply_hamiltonian(ctx, psi->d(), lam->d(), n, nb, d_terms.as<PauliTermDev>(),
+                                     static_cast<uint32_t>(terms.size()));
+        }
+        launch_batched_inner_re_p(ctx, psi->d(), lam->d(), n, nb, d_part.as<double>(),
+                                  d_energy.as<double>());
+        for (size_t i = steps.size(); i-- > 0;) {
+            const GateStep& s = steps[i];
+            if (s.param >= 0) {
+                launch_batched_pauli_im_p(ctx, lam->d(), psi->d(), n, nb, s.gen.x, s.gen.zy,
+                                          s.gen.n_y, d_part.as<double>(),
+                                          d_grad.as<double>() + s.param, np);
+                const double2* inv = d_csi.as<double2>() + static_cast<uint64_t>(s.param) * R;
+                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+                launch_pauli_rotation_batched(ctx, lam->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+            } else {
+                s.inv.launch(ctx, psi->d(), n, nb);
+                s.inv.launch(ctx, lam->d(), n, nb);
+            }
+        }
+    }
+
+    void run(uint32_t nb) {
+        const char* e = std::getenv("LQCS_GRAPHS");
+        if (e && e[0] == '0') {
+            enqueue(nb);
+            return;
+        }
+        auto it = graphs.find(nb);
+        bool fresh = false;
+        if (it == graphs.end()) {
+            // capture once; a failed capture falls back to direct launches (which rethrow any
+            // real launch error)
+            const uint64_t k0 = launch_count();
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            bool ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                try {
+                    enqueue(nb);
+                } catch (...) {
+                    ok = false;
+                }
+                cudaGraph_t done = nullptr;
+                const bool ended = cudaStreamEndCapture(stream, &done) == cudaSuccess;
+                g = done;
+                ok = ok && ended && g;
+            }
+            if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            if (!ok) {
+                cudaGetLastError();
+                enqueue(nb);
+                return;
+            }
+            it = graphs.emplace(nb, std::make_pair(exec, launch_count() - k0)).first;
+            fresh = true;   // the capture already counted this batch's kernels
+        }
+        cuda_check(cudaGraphLaunch(it->second.first, stream), "cudaGraphLaunch");
+        if (!fresh) count_launch(it->second.second);   // the graph's kernels, each replay
+    }
+};
+
+uint64_t plan_key(const std::vector<GateDesc>& tmpl, const std::vector<int>& param_of,
+                  const Hamiltonian& h, uint32_t n, uint32_t R) {
+    uint64_t k = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t len) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < len; ++i) k = (k ^ b[i]) * 1099511628211ull;
+    };
+    mix(&n, sizeof n);
+    mix(&R, sizeof R);
+    for (size_t i = 0; i < tmpl.size(); ++i) {
+        const GateDesc& g = tmpl[i];
+        mix(&g.type, sizeof g.type);
+        mix(&g.n_controls, sizeof g.n_controls);
+        mix(g.qubits.data(), g.qubits.size() * sizeof(uint32_t));
+        mix(&param_of[i], sizeof(int));
+        if (param_of[i] < 0) {   // fixed gates: their values are part of the plan
+            mix(g.params.data(), g.params.size() * sizeof(double));
+            mix(g.mat.data(), g.mat.size() * sizeof(cd));
+            mix(g.perm.data(), g.perm.size() * sizeof(uint64_t));
+        }
+        mix(g.pauli.data(), g.pauli.size());
+    }
+    for (size_t t = 0; t < h.terms.size(); ++t) {
+        mix(&h.terms[t].x, sizeof(uint64_t));
+        mix(&h.terms[t].zy, sizeof(uint64_t));
+        mix(&h.coeffs[t], sizeof(double));
+    }
+    return k;
+}
+
+// The most recent plans (resident memory: two state batches each), newest last.
+std::mutex g_plan_mu;
+std::vector<std::unique_ptr<AdjointPlan>> g_plans;
+constexpr size_t kKeptPlans = 2;
+
+AdjointPlan& adjoint_plan(const std::vector<GateDesc>& tmpl, const std::vector<int>& param_of,
+                          const Hamiltonian& h, uint32_t n, uint64_t np, uint64_t batch,
+                          uint32_t max_resident) {
+    const uint32_t R = max_resident ? static_cast<uint32_t>(std::min<uint64_t>(max_resident, batch))
+                                    : default_resident(n, batch);
+    const uint64_t key = plan_key(tmpl, param_of, h, n, R);
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    const uint64_t dkey = key ^ (static_cast<uint64_t>(dev) << 56);
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    for (auto& p : g_plans)
+        if (p->key == dkey) return *p;
+    auto plan = std::make_unique<AdjointPlan>();
+    plan->key = dkey;
+    plan->n = n;
+    plan->R = R;
+    plan->np = np;
+    cuda_check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // the fixed gates (and their inverses); barrier / measure are skipped
+    for (size_t i = 0; i < tmpl.size(); ++i) {
+        const GateDesc& g = tmpl[i];
+        if (g.type == LQCS_GATE_RESET) invalid("run_statevector: Reset is non-deterministic; use run() instead");
+        if (!g.is_unitary()) continue;
+        GateStep s;
+        s.param = param_of[i];
+        if (s.param >= 0) {
+            s.gen = generator(g);
+        } else {
+            const DevOp op = lower_gate(g, n);
+            s.fwd.build({op}, plan->stream);
+            s.inv.build({invert(op)}, plan->stream);
+        }
+        plan->steps.push_back(std::move(s));
+    }
+    plan->psi = new_state(n, R, plan->stream);
+    plan->lam = new_state(n, R, plan->stream);
+    static const cd ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+    for (size_t t = 0; t < h.terms.size(); ++t) {
+        const cd c = h.coeffs[t] * ipow[h.terms[t].n_y % 4];
+        plan->terms.push_back({h.terms[t].x, h.terms[t].zy, make_double2(c.real(), c.imag())});
+    }
+    plan->d_terms.ensure(sizeof(PauliTermDev) * std::max<size_t>(1, plan->terms.size()));
+    if (!plan->terms.empty())
+        cuda_check(cudaMemcpy(plan->d_terms.ptr, plan->terms.data(),
+                              sizeof(PauliTermDev) * plan->terms.size(), cudaMemcpyHostToDevice),
+                   "H2D terms");
+    plan->d_cs.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
+    plan->d_csi.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
+    plan->d_part.ensure(sizeof(double) * 64 * R);
+    plan->d_energy.ensure(sizeof(double) * R);
+    plan->d_grad.ensure(sizeof(double) * std::max<uint64_t>(1, np) * R);
+    if (g_plans.size() >= kKeptPlans) g_plans.erase(g_plans.begin());
+    g_plans.push_back(std::move(plan));
+    return *g_plans.back();
+}
+
+}  // namespace
+
 void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
                      const double* params, uint64_t batch, uint32_t max_resident,
                      double* energy_out, double* grad_out) {
@@ -165,50 +368,10 @@ void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
         return;
     }
 
-    // Precompile the fixed gates (and their inverses); barrier/measure are skipped.
-    std::vector<GateStep> steps;
-    steps.reserve(tmpl.size());
-    for (size_t i = 0; i < tmpl.size(); ++i) {
-        const GateDesc& g = tmpl[i];
-        if (g.type == LQCS_GATE_RESET) invalid("run_statevector: Reset is non-deterministic; use run() instead");
-        if (!g.is_unitary()) continue;
-        GateStep s;
-        s.param = param_of[i];
-        if (s.param >= 0) {
-            s.gen = generator(g);
-        } else {
-            const DevOp op = lower_gate(g, n);
-            s.fwd.build({op}, nullptr);
-            s.inv.build({invert(op)}, nullptr);
-        }
-        steps.push_back(std::move(s));
-    }
-
-    const uint32_t R = max_resident ? static_cast<uint32_t>(std::min<uint64_t>(max_resident, batch))
-                                    : default_resident(n, batch);
-    auto psi = new_state(n, R, nullptr);
-    auto lam = new_state(n, R, nullptr);
-    const LaunchCtx ctx = psi->ctx;
-
-    std::vector<PauliTermDev> terms;
-    static const cd ipow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
-    for (size_t t = 0; t < h.terms.size(); ++t) {
-        const cd c = h.coeffs[t] * ipow[h.terms[t].n_y % 4];
-        terms.push_back({h.terms[t].x, h.terms[t].zy, make_double2(c.real(), c.imag())});
-    }
-    DeviceBuffer d_terms, d_cs, d_csi, d_part, d_energy, d_grad;
-    d_terms.ensure(sizeof(PauliTermDev) * std::max<size_t>(1, terms.size()));
-    if (!terms.empty())
-        cuda_check(cudaMemcpy(d_terms.ptr, terms.data(), sizeof(PauliTermDev) * terms.size(),
-                              cudaMemcpyHostToDevice), "H2D terms");
-    d_cs.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
-    d_csi.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
-    d_part.ensure(sizeof(double) * 64 * R);
-    d_energy.ensure(sizeof(double) * R);
-    d_grad.ensure(sizeof(double) * std::max<uint64_t>(1, np) * R);
+    AdjointPlan& plan = adjoint_plan(tmpl, param_of, h, n, np, batch, max_resident);
+    const uint32_t R = plan.R;
     std::vector<double2> cs(np * R), csi(np * R);
     std::vector<double> h_energy(R), h_grad(np * R);
-
     for (uint64_t b0 = 0; b0 < batch; b0 += R) {
         const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(R, batch - b0));
         // (cos, sin) of theta/2 per parameter and set; layout [param][set]
@@ -220,46 +383,18 @@ void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
             }
         }
         if (np) {
-            cuda_check(cudaMemcpy(d_cs.ptr, cs.data(), sizeof(double2) * np * R, cudaMemcpyHostToDevice), "H2D");
-            cuda_check(cudaMemcpy(d_csi.ptr, csi.data(), sizeof(double2) * np * R, cudaMemcpyHostToDevice), "H2D");
+            cuda_check(cudaMemcpyAsync(plan.d_cs.ptr, cs.data(), sizeof(double2) * np * R,
+                                       cudaMemcpyHostToDevice, plan.stream), "H2D");
+            cuda_check(cudaMemcpyAsync(plan.d_csi.ptr, csi.data(), sizeof(double2) * np * R,
+                                       cudaMemcpyHostToDevice, plan.stream), "H2D");
         }
-        launch_set_basis(ctx, psi->d(), n, nb, 0);
-        for (const GateStep& s : steps) {
-            if (s.param >= 0) {
-                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y,
-                                              d_cs.as<double2>() + static_cast<uint64_t>(s.param) * R);
-            } else {
-                s.fwd.launch(ctx, psi->d(), n, nb);
-            }
-        }
-        if (terms.empty()) {
-            cuda_check(cudaMemsetAsync(lam->d(), 0, sizeof(double2) * len * nb, ctx.stream), "memset");
-        } else {
-            launch_apply_hamiltonian(ctx, psi->d(), lam->d(), n, nb, d_terms.as<PauliTermDev>(),
-                                     static_cast<uint32_t>(terms.size()));
-        }
-        launch_batched_inner_re_p(ctx, psi->d(), lam->d(), n, nb, d_part.as<double>(),
-                                  d_energy.as<double>());
-        for (size_t i = steps.size(); i-- > 0;) {
-            const GateStep& s = steps[i];
-            if (s.param >= 0) {
-                launch_batched_pauli_im_p(ctx, lam->d(), psi->d(), n, nb, s.gen.x, s.gen.zy,
-                                          s.gen.n_y, d_part.as<double>(),
-                                          d_grad.as<double>() + s.param, np);
-                const double2* inv = d_csi.as<double2>() + static_cast<uint64_t>(s.param) * R;
-                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
-                launch_pauli_rotation_batched(ctx, lam->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
-            } else {
-                s.inv.launch(ctx, psi->d(), n, nb);
-                s.inv.launch(ctx, lam->d(), n, nb);
-            }
-        }
-        cuda_check(cudaMemcpyAsync(h_energy.data(), d_energy.ptr, sizeof(double) * nb,
-                                   cudaMemcpyDeviceToHost, ctx.stream), "D2H energies");
+        plan.run(nb);
+        cuda_check(cudaMemcpyAsync(h_energy.data(), plan.d_energy.ptr, sizeof(double) * nb,
+                                   cudaMemcpyDeviceToHost, plan.stream), "D2H energies");
         if (np)
-            cuda_check(cudaMemcpyAsync(h_grad.data(), d_grad.ptr, sizeof(double) * np * nb,
-                                       cudaMemcpyDeviceToHost, ctx.stream), "D2H gradients");
-        cuda_check(cudaStreamSynchronize(ctx.stream), "adjoint");
+            cuda_check(cudaMemcpyAsync(h_grad.data(), plan.d_grad.ptr, sizeof(double) * np * nb,
+                                       cudaMemcpyDeviceToHost, plan.stream), "D2H gradients");
+        cuda_check(cudaStreamSynchronize(plan.stream), "adjoint");
         for (uint32_t b = 0; b < nb; ++b) {
             if (energy_out) energy_out[b0 + b] = h_energy[b];
             if (grad_out)
