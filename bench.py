@@ -222,6 +222,37 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ CPU baseline leg
+def cpu_side_baselines(ref) -> dict:
+    """The reference's own CPU methods for the batched legs, on bounded samples (same run,
+    all host cores): the parameter-shift gradient of one config-2 parameter set, and one
+    config-3 trajectory over the first 2 of its 20 layers (scaled by 10, stated)."""
+    from litequantumcomputingsimulator_b200 import workloads as W
+    out = {}
+    try:
+        pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+        ham = W.random_hamiltonian(16, 500, seed=12)
+        sets = W.random_parameter_sets(pc.num_parameters(), 1, seed=13)
+        t0 = time.perf_counter()
+        ref.parameter_shift_gradient(ham, pc, sets[0])
+        dt = time.perf_counter() - t0
+        out["config2_parameter_shift_s_per_set"] = dt
+        out["config2_parameter_shift_grads_per_s"] = 1.0 / dt
+    except Exception as ex:  # noqa: BLE001
+        out["config2_error"] = str(ex)
+    try:
+        tq = W.brickwork(26, 2, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+        t0 = time.perf_counter()
+        ref.trajectories(tq, 1, 404)
+        dt = time.perf_counter() - t0
+        out["config3_trajectory_s_2_layers"] = dt
+        out["config3_trajectories_per_s_est"] = 1.0 / (dt * 10)
+        out["config3_sample"] = ("one 26-qubit trajectory over 2 of 20 layers (reference-semantics "
+                                 "driver on the reference kernels), x10 for the full depth")
+    except Exception as ex:  # noqa: BLE001
+        out["config3_error"] = str(ex)
+    return out
+
+
 def cpu_baseline(n: int, qc, budget_s: float = 12.0) -> dict:
     from oracle.oracle import Ref, Port
     import litequantumcomputingsimulator_b200 as lq
@@ -239,10 +270,12 @@ def cpu_baseline(n: int, qc, budget_s: float = 12.0) -> dict:
         for inst in insts[:g]:
             sample.append(inst)
         t = ref.time_apply(sample, 1)
-        return {"value": W.alg_bytes(sample) / t / 1e9, "unit": UNIT, "cores": cores,
-                "kind": "reference",
-                "sample": f"first {g} gates of the {n}-qubit brickwork, reference OpenMP kernels, "
-                          f"{t:.2f} s"}
+        out = {"value": W.alg_bytes(sample) / t / 1e9, "unit": UNIT, "cores": cores,
+               "kind": "reference",
+               "sample": f"first {g} gates of the {n}-qubit brickwork, reference OpenMP kernels, "
+                         f"{t:.2f} s"}
+        out.update(cpu_side_baselines(ref))
+        return out
     # the scalar port on a 26-qubit sample, one core
     m = min(n, 26)
     port = Port()
@@ -572,7 +605,15 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
                      [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14)]]
         t0 = time.perf_counter()
         x, y = CM.collect(train_set)
+        t1 = time.perf_counter()
         loss = CM.train(x, y, epochs=3000, lr=3e-3, seed=0)
+        t_train = time.perf_counter() - t1
+        out["costmodel_train_rows_x_epochs_per_s"] = y.size * 3000 / t_train
+        xi = np.repeat(x, max(1, 1_000_000 // max(1, len(x))), axis=0)
+        CM.predict(xi[:1024])
+        t1 = time.perf_counter()
+        CM.predict(xi)
+        out["costmodel_infer_rows_per_s"] = len(xi) / (time.perf_counter() - t1)
         out["costmodel_train_rows"] = int(y.size)
         out["costmodel_train_mse"] = loss
         out["costmodel_collect_train_s"] = time.perf_counter() - t0

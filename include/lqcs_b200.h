@@ -219,6 +219,23 @@ int lqcs_run(uint32_t n_qubits, uint32_t n_clbits, const lqcs_instruction* insts
              uint64_t n_insts, uint64_t shots, const lqcs_sim_options* opts,
              uint64_t* shot_registers);
 
+/* ------------------------------------------------------------------ density matrices
+ * DensityMatrixSimulator (src/backend/density_matrix_simulator.cpp) on the device.  rho of
+ * n qubits lives in a state handle of 2n qubits: element rho_{rc} at index (c << n) | r
+ * (DensityMatrix::element, src/backend/density_matrix.cpp).  Each unitary is applied as U on
+ * the ket bits and conj(U) on the bra bits, each channel of opts->channels follows every
+ * unitary on each qubit it touches, explicit Kraus instructions apply where they stand;
+ * Measure and Barrier are skipped, Reset is rejected (as the reference). */
+int lqcs_dm_create(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                   const lqcs_sim_options* opts, lqcs_state** out);   /* run_density_matrix */
+/* Diagonal rho_ii of a density-matrix handle (2^n doubles): DensityMatrix::probabilities. */
+int lqcs_dm_probabilities(const lqcs_state* rho, double* probs);
+/* DensityMatrixSimulator::run: terminal measurements only; one register per shot as
+ * lqcs_run, drawn from the diagonal with the same uniforms and upper_bound rule. */
+int lqcs_dm_run(uint32_t n_qubits, uint32_t n_clbits, const lqcs_instruction* insts,
+                uint64_t n_insts, uint64_t shots, const lqcs_sim_options* opts,
+                uint64_t* shot_registers);
+
 /* Read `count` amplitudes starting at basis index `first` (of state 0) into host memory
  * (2*count doubles).  Serves Statevector::operator[] (include/lqcs/backend/statevector.hpp:21-22). */
 int lqcs_state_read_range(const lqcs_state* st, uint64_t first, uint64_t count, double* host);

@@ -17,11 +17,14 @@ Quick start::
 from . import algorithms
 from .circuit import Gate, GateType, Instruction, ParametricCircuit, QuantumCircuit
 from .noise import KrausChannel, NoiseModel
-from .simulator import Result, Statevector, StatevectorSimulator
+from .simulator import (DensityMatrix, DensityMatrixSimulator, Result, Statevector,
+                        StatevectorSimulator)
 
 __version__ = "0.1.0"
 
 __all__ = [
+    "DensityMatrix",
+    "DensityMatrixSimulator",
     "Gate",
     "GateType",
     "Instruction",

@@ -164,6 +164,11 @@ SIGNATURES = {
     "lqcs_rng_uniforms": (C.c_int, [C.c_uint64, C.c_uint64, C.c_void_p]),
     "lqcs_autotune": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_uint64,
                                 _P(TuneEntry), _P(C.c_uint64)]),
+    "lqcs_dm_create": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, _P(SimOptions),
+                                 _P(StatePtr)]),
+    "lqcs_dm_probabilities": (C.c_int, [StatePtr, C.c_void_p]),
+    "lqcs_dm_run": (C.c_int, [C.c_uint32, C.c_uint32, _P(Instruction), C.c_uint64, C.c_uint64,
+                              _P(SimOptions), C.c_void_p]),
     "lqcs_costmodel_features": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_uint32, C.c_uint32, C.c_void_p]),
     "lqcs_costmodel_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_float,

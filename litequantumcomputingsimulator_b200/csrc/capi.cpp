@@ -226,6 +226,37 @@ int lqcs_run(uint32_t n_qubits, uint32_t n_clbits, const lqcs_instruction* insts
     });
 }
 
+int lqcs_dm_create(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
+                   const lqcs_sim_options* opts, lqcs_state** out) {
+    return guarded([&] {
+        need(out, "out");
+        *out = nullptr;
+        if (n_qubits == 0) lqcs_b200::invalid("DensityMatrix: num_qubits must be >= 1");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        *out = lqcs_b200::dm_evolve(n_qubits, gates, opts).release();
+    });
+}
+
+int lqcs_dm_probabilities(const lqcs_state* rho, double* probs) {
+    return guarded([&] {
+        need(rho, "rho");
+        need(probs, "probs");
+        if (rho->n % 2 != 0 || rho->batch != 1) lqcs_b200::invalid("dm_probabilities: not a density matrix");
+        lqcs_b200::dm_probabilities(const_cast<lqcs_state&>(*rho), rho->n / 2, probs);
+    });
+}
+
+int lqcs_dm_run(uint32_t n_qubits, uint32_t n_clbits, const lqcs_instruction* insts,
+                uint64_t n_insts, uint64_t shots, const lqcs_sim_options* opts,
+                uint64_t* shot_registers) {
+    return guarded([&] {
+        if (n_qubits == 0) lqcs_b200::invalid("QuantumCircuit: num_qubits must be >= 1");
+        if (shots > 0) need(shot_registers, "shot_registers");
+        const auto gates = lqcs_b200::decode_all(insts, n_insts, n_qubits);
+        lqcs_b200::dm_run_shots(n_qubits, n_clbits, gates, shots, opts, shot_registers);
+    });
+}
+
 int lqcs_state_read_range(const lqcs_state* st, uint64_t first, uint64_t count, double* host) {
     return guarded([&] {
         need(st, "state");

@@ -757,12 +757,10 @@ void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, doub
 
 // ------------------------------------------------------------------ run()
 
-namespace {
-
 using Kraus = std::array<cd, 4>;
 using Channel = std::vector<Kraus>;
 
-std::vector<Channel> decode_channels(const lqcs_sim_options* opts) {
+std::vector<std::vector<std::array<cd, 4>>> decode_channels(const lqcs_sim_options* opts) {
     std::vector<Channel> out;
     if (!opts || opts->n_channels == 0) return out;
     if (!opts->channels) invalid("NoiseModel: channels pointer is null");
@@ -776,6 +774,8 @@ std::vector<Channel> decode_channels(const lqcs_sim_options* opts) {
     }
     return out;
 }
+
+namespace {
 
 // Emission order of SingleQubitGateFusion (src/transpiler/gate_fusion.cpp:32-67), reduced
 // to what run()'s path selection reads from it: true when some unitary is emitted after a

@@ -148,6 +148,16 @@ using Rng = std::mt19937_64;
 // std::uniform_real_distribution<double>(0, 1) over std::mt19937_64.
 double rng_uniform(Rng& r);
 Rng make_rng(const lqcs_sim_options* opts);
+// NoiseModel channels of the options (each a list of 2x2 Kraus operators).
+std::vector<std::vector<std::array<cd, 4>>> decode_channels(const lqcs_sim_options* opts);
+
+// Density-matrix backend (dm.cpp): rho of n qubits as a 2n-qubit device state, element
+// rho_{rc} at (c << n) | r.
+std::unique_ptr<lqcs_state> dm_evolve(uint32_t n, const std::vector<GateDesc>& gates,
+                                      const lqcs_sim_options* opts);
+void dm_probabilities(lqcs_state& rho, uint32_t n, double* host);
+void dm_run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,
+                  uint64_t shots, const lqcs_sim_options* opts, uint64_t* regs);
 
 std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t stream);
 uint32_t max_qubits_on_device(uint32_t batch);

@@ -117,6 +117,11 @@ void launch_probabilities(const LaunchCtx& ctx, const double2* st, uint32_t n, d
 uint64_t scan_block_count(uint32_t n);
 void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_cum,
                       double* d_block);
+// The same over the diagonal rho_ii of an n-qubit density matrix held as a 2n-qubit vector
+// (element (col << n) | row), and the diagonal itself (2^n doubles).
+void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_cum,
+                         double* d_block);
+void launch_dm_diagonal(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_p);
 // upper_bound(cum, u_s * cum[N-1]) per shot; d_margin[s] = distance to the nearest edge / total
 void launch_sample_search(const LaunchCtx& ctx, const double* d_cum, uint32_t n,
                           const double* d_u, uint64_t shots, uint64_t* d_idx,

@@ -300,8 +300,21 @@ uint64_t scan_block_count(uint32_t n) {
     return (len + kSegAmps - 1) / kSegAmps;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_seg(const double2* __restrict__ s,
-                                                           uint64_t len, double* __restrict__ cum,
+// Probability sources of the scan: |a_i|^2 of a statevector, or the diagonal rho_ii of a
+// density matrix stored as a 2n-qubit vector (element (col << n) | row).
+struct AmpSource {
+    const double2* s;
+    __device__ double operator()(uint64_t i) const { return norm_rn(__ldg(s + i)); }
+};
+struct DiagSource {
+    const double2* rho;
+    uint32_t n;
+    __device__ double operator()(uint64_t i) const { return __ldg(rho + ((i << n) | i)).x; }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(kScanThreads) k_scan_seg(Src src, uint64_t len,
+                                                           double* __restrict__ cum,
                                                            double* __restrict__ seg_total) {
     __shared__ double tsum[kScanThreads];
     const uint64_t seg0 = static_cast<uint64_t>(blockIdx.x) * kSegAmps;
@@ -311,7 +324,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_seg(const double2* __rest
 #pragma unroll
     for (uint32_t k = 0; k < kPerThread; ++k) {
         const uint64_t i = i0 + k;
-        const double p = (i < len) ? norm_rn(__ldg(s + i)) : 0.0;
+        const double p = (i < len) ? src(i) : 0.0;
         acc = (k == 0) ? p : __dadd_rn(acc, p);
         local[k] = acc;
     }
@@ -378,12 +391,12 @@ __global__ void k_scan_add(double* __restrict__ cum, uint64_t len,
     }
 }
 
-void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_cum,
-                      double* d_block) {
+template <class Src>
+void prob_scan(const LaunchCtx& ctx, Src src, uint32_t n, double* d_cum, double* d_block) {
     const uint64_t len = uint64_t{1} << n;
     const uint64_t nseg = scan_block_count(n);
-    k_scan_seg<<<static_cast<uint32_t>(nseg), kScanThreads, 0, ctx.stream>>>(st, len, d_cum,
-                                                                             d_block);
+    k_scan_seg<Src><<<static_cast<uint32_t>(nseg), kScanThreads, 0, ctx.stream>>>(src, len, d_cum,
+                                                                                  d_block);
     check_launch("scan_seg");
     if (nseg > 1) {
         k_scan_top<<<1, 1024, 0, ctx.stream>>>(d_block, nseg);
@@ -393,6 +406,32 @@ void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, doubl
         k_scan_add<<<nb, 256, 0, ctx.stream>>>(d_cum, len, d_block);
         check_launch("scan_add");
     }
+}
+
+void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_cum,
+                      double* d_block) {
+    prob_scan(ctx, AmpSource{st}, n, d_cum, d_block);
+}
+
+void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_cum,
+                         double* d_block) {
+    prob_scan(ctx, DiagSource{rho, n}, n, d_cum, d_block);
+}
+
+__global__ void k_dm_diag(const double2* __restrict__ rho, uint32_t n, double* __restrict__ p) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < len;
+         i += stride)
+        p[i] = __ldg(rho + ((i << n) | i)).x;
+}
+
+void launch_dm_diagonal(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_p) {
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(
+        (len + 255) / 256, static_cast<uint64_t>(ctx.num_sms) * 8));
+    k_dm_diag<<<std::max(1u, nb), 256, 0, ctx.stream>>>(rho, n, d_p);
+    check_launch("dm_diag");
 }
 
 // std::upper_bound(cum, cum + N, u * total) for every shot

@@ -308,3 +308,71 @@ class StatevectorSimulator:
         N.call("lqcs_run", circuit.num_qubits(), circuit.num_clbits(), arr, n, int(shots),
                C.byref(opts), regs.ctypes.data)
         return regs[:shots]
+
+
+class DensityMatrix:
+    """lqcs::DensityMatrix (include/lqcs/backend/density_matrix.hpp) held on the device as a
+    2n-qubit vector: element rho_{rc} at index (c << n) | r."""
+
+    def __init__(self, state: Statevector, num_qubits: int):
+        self._sv = state
+        self._n = int(num_qubits)
+
+    def num_qubits(self) -> int:
+        return self._n
+
+    def dim(self) -> int:
+        return 1 << self._n
+
+    def probabilities(self) -> np.ndarray:
+        out = np.empty(self.dim(), dtype=np.float64)
+        N.call("lqcs_dm_probabilities", self._sv.handle, out.ctypes.data)
+        return out
+
+    def to_numpy(self) -> np.ndarray:
+        """rho as a dim x dim host matrix."""
+        d = self.dim()
+        return self._sv.to_numpy().reshape(d, d).T.copy()
+
+    def element(self, row: int, col: int) -> complex:
+        d = self.dim()
+        if not (0 <= row < d and 0 <= col < d):
+            raise IndexError("DensityMatrix::element: index out of range")
+        return complex(self._sv[(col << self._n) | row])
+
+    def trace(self) -> float:
+        return float(self.probabilities().sum())
+
+    def purity(self) -> float:
+        """Tr(rho^2) = sum |rho_rc|^2 (rho Hermitian)."""
+        return float(self._sv.norm() ** 2)
+
+
+class DensityMatrixSimulator:
+    """Drop-in for lqcs::DensityMatrixSimulator (seed, noise): run() samples the final
+    diagonal (terminal measurements only), run_density_matrix() returns rho."""
+
+    def __init__(self, seed: Optional[int] = None, noise: Optional[NoiseModel] = None):
+        self._sim = StatevectorSimulator(seed=seed, noise=noise)
+
+    def name(self) -> str:
+        return "density_matrix_simulator"
+
+    def run_density_matrix(self, circuit: QuantumCircuit) -> DensityMatrix:
+        opts, keep = self._sim._options()
+        arr, n, _k = circuit.c_instructions()
+        h = N.StatePtr()
+        N.call("lqcs_dm_create", circuit.num_qubits(), arr, n, C.byref(opts), C.byref(h))
+        return DensityMatrix(Statevector(_handle=h), circuit.num_qubits())
+
+    def run_registers(self, circuit: QuantumCircuit, shots: int = 1024) -> np.ndarray:
+        opts, keep = self._sim._options()
+        arr, n, _k = circuit.c_instructions()
+        regs = np.zeros(max(int(shots), 1), dtype=np.uint64)
+        N.call("lqcs_dm_run", circuit.num_qubits(), circuit.num_clbits(), arr, n, int(shots),
+               C.byref(opts), regs.ctypes.data)
+        return regs[:shots]
+
+    def run(self, circuit: QuantumCircuit, shots: int = 1024) -> Result:
+        return Result(registers_to_counts(self.run_registers(circuit, shots), circuit.num_clbits()),
+                      shots)

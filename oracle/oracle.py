@@ -537,6 +537,7 @@ class Ref:
                 "lqcsref_max_threads": (i, []),
                 "lqcsref_run_statevector": (i, [u32, vp, u64, i, vp]),
                 "lqcsref_run": (i, [u32, u32, vp, u64, u64, i, u64, i, u64, vp, vp, vp, u64, vp]),
+                "lqcsref_dm_run": (i, [u32, u32, vp, u64, u64, i, u64, u64, vp, vp, vp, u64, vp]),
                 "lqcsref_evolve_from": (i, [u32, vp, vp, u64, vp]),
                 "lqcsref_time_apply": (i, [u32, vp, u64, u32, vp]),
                 "lqcsref_expectation": (i, [u32, vp, C.c_char_p, vp]),
@@ -584,6 +585,22 @@ class Ref:
                                          int(fuse), nch, C.cast(chp, C.c_void_p) if chp else None,
                                          keys.ctypes.data, counts.ctypes.data, keys.size,
                                          C.byref(nout)))
+        return {int(k): int(c) for k, c in zip(keys[: nout.value], counts[: nout.value])}
+
+    def dm_run(self, circuit, shots: int, seed: Optional[int], noise=None) -> dict:
+        """DensityMatrixSimulator::run counts {register int: count}."""
+        arr, n, _k = circuit.c_instructions()
+        chp, nch, keep = (noise.c_channels() if noise is not None else (None, 0, []))
+        cap = 1 << 20
+        keys = np.zeros(min(cap, max(shots, 1)), dtype=np.uint64)
+        counts = np.zeros_like(keys)
+        nout = C.c_uint64(0)
+        self._check(self.lib.lqcsref_dm_run(circuit.num_qubits(), circuit.num_clbits(),
+                                            C.cast(arr, C.c_void_p), n, shots,
+                                            0 if seed is None else 1, 0 if seed is None else seed,
+                                            nch, C.cast(chp, C.c_void_p) if chp else None,
+                                            keys.ctypes.data, counts.ctypes.data, keys.size,
+                                            C.byref(nout)))
         return {int(k): int(c) for k, c in zip(keys[: nout.value], counts[: nout.value])}
 
     def evolve_from(self, circuit, state: np.ndarray) -> np.ndarray:

@@ -215,6 +215,22 @@ int lqcsref_run(uint32_t n, uint32_t nclbits, const lqcs_instruction* insts, uin
     });
 }
 
+// DensityMatrixSimulator::run (src/backend/density_matrix_simulator.cpp:26-80): counts of
+// the final density matrix's diagonal, noise model after every unitary.
+int lqcsref_dm_run(uint32_t n, uint32_t nclbits, const lqcs_instruction* insts, uint64_t n_insts,
+                   uint64_t shots, int has_seed, uint64_t seed, uint64_t n_channels,
+                   const lqcs_kraus_channel* channels, uint64_t* keys, uint64_t* counts,
+                   uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        DensityMatrixSimulator::Options o;
+        if (has_seed) o.seed = seed;
+        for (uint64_t c = 0; c < n_channels; ++c) o.noise.add_all_qubit_channel(to_channel(channels[c]));
+        DensityMatrixSimulator sim(o);
+        const Result r = sim.run(to_circuit(n, nclbits, insts, n_insts), shots);
+        write_counts(r, keys, counts, cap, n_out);
+    });
+}
+
 // Evolve a given state by the unitary instructions with the reference kernels.
 int lqcsref_evolve_from(uint32_t n, const double* in, const lqcs_instruction* insts,
                         uint64_t n_insts, double* out) {
