@@ -240,6 +240,13 @@ def cpu_side_baselines(ref) -> dict:
     except Exception as ex:  # noqa: BLE001
         out["config2_error"] = str(ex)
     try:
+        dq = W.brickwork(10, 20, seed=88, noise=(1e-3, 1e-2, 1e-3))
+        t0 = time.perf_counter()
+        ref.dm_probabilities(dq)
+        out["dm_10q_d20_reference_s"] = time.perf_counter() - t0
+    except Exception as ex:  # noqa: BLE001
+        out["dm_reference_error"] = str(ex)
+    try:
         tq = W.brickwork(26, 2, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
         t0 = time.perf_counter()
         ref.trajectories(tq, 1, 404)
@@ -595,6 +602,21 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["autotune_28q_gain_vs_default"] = default[0]["ms"] / chosen[0]["ms"]
     except Exception as ex:  # noqa: BLE001
         out["autotune_error"] = str(ex)
+
+    # density-matrix backend: config-3 noise on a 13-qubit brickwork, depth 20 (rho as a
+    # 26-qubit device state, 1 GiB), and the 10-qubit cross-check size
+    try:
+        for nq in (10, 13):
+            dq = W.brickwork(nq, 20, seed=88, noise=(1e-3, 1e-2, 1e-3))
+            dsim = lq.DensityMatrixSimulator()
+            dsim.run_density_matrix(W.brickwork(nq, 1, seed=1))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p = dsim.run_density_matrix(dq).probabilities()
+            out[f"dm_{nq}q_d20_s"] = time.perf_counter() - t0
+            out[f"dm_{nq}q_trace"] = float(p.sum())
+    except Exception as ex:  # noqa: BLE001
+        out["dm_error"] = str(ex)
 
     # learned fusion cost model: trained on the engine's own per-operation timings of
     # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the

@@ -14,7 +14,7 @@ Quick start::
     qc.h(0).cx(0, 1).measure_all()
     print(lq.StatevectorSimulator(seed=42).run(qc, shots=1024).counts())
 """
-from . import algorithms
+from . import algorithms, io
 from .circuit import Gate, GateType, Instruction, ParametricCircuit, QuantumCircuit
 from .noise import KrausChannel, NoiseModel
 from .simulator import (DensityMatrix, DensityMatrixSimulator, Result, Statevector,
@@ -36,4 +36,5 @@ __all__ = [
     "Statevector",
     "StatevectorSimulator",
     "algorithms",
+    "io",
 ]

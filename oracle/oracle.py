@@ -538,6 +538,7 @@ class Ref:
                 "lqcsref_run_statevector": (i, [u32, vp, u64, i, vp]),
                 "lqcsref_run": (i, [u32, u32, vp, u64, u64, i, u64, i, u64, vp, vp, vp, u64, vp]),
                 "lqcsref_dm_run": (i, [u32, u32, vp, u64, u64, i, u64, u64, vp, vp, vp, u64, vp]),
+                "lqcsref_qasm_roundtrip": (i, [C.c_char_p, vp, u64]),
                 "lqcsref_evolve_from": (i, [u32, vp, vp, u64, vp]),
                 "lqcsref_time_apply": (i, [u32, vp, u64, u32, vp]),
                 "lqcsref_expectation": (i, [u32, vp, C.c_char_p, vp]),
@@ -602,6 +603,13 @@ class Ref:
                                             keys.ctypes.data, counts.ctypes.data, keys.size,
                                             C.byref(nout)))
         return {int(k): int(c) for k, c in zip(keys[: nout.value], counts[: nout.value])}
+
+    def qasm_roundtrip(self, source: str) -> str:
+        """io::to_qasm(io::from_qasm(source)) of the reference."""
+        buf = C.create_string_buffer(1 << 22)
+        self._check(self.lib.lqcsref_qasm_roundtrip(source.encode(), C.cast(buf, C.c_void_p),
+                                                    len(buf)))
+        return buf.value.decode()
 
     def evolve_from(self, circuit, state: np.ndarray) -> np.ndarray:
         arr, n, _k = circuit.c_instructions()

@@ -231,6 +231,15 @@ int lqcsref_dm_run(uint32_t n, uint32_t nclbits, const lqcs_instruction* insts, 
     });
 }
 
+// io::to_qasm(io::from_qasm(src)) (src/io/qasm.cpp) into out (capacity cap, NUL-terminated).
+int lqcsref_qasm_roundtrip(const char* src, char* out, uint64_t cap) {
+    return guarded([&] {
+        const std::string text = io::to_qasm(io::from_qasm(src));
+        if (text.size() + 1 > cap) throw std::invalid_argument("qasm_roundtrip: buffer too small");
+        std::memcpy(out, text.c_str(), text.size() + 1);
+    });
+}
+
 // Evolve a given state by the unitary instructions with the reference kernels.
 int lqcsref_evolve_from(uint32_t n, const double* in, const lqcs_instruction* insts,
                         uint64_t n_insts, double* out) {
