@@ -99,7 +99,10 @@ typedef struct lqcs_kraus_channel {
  *   fusion_mode      : 0 = default planner, 1 = greedy, 2 = learned cost model,
  *                      3 = gate-by-gate (no fusion even if fuse_gates), 4 = tile passes,
  *                      5 = autotuned (lqcs_autotune's measured choice)
- *   max_resident     : most noise trajectories held on the device at once. */
+ *   max_resident     : most noise trajectories held on the device at once.
+ *   shot_offset      : the call's shots are shots shot_offset.. of a longer run with the same
+ *                      seed: the uniforms of the shots before them are skipped, so runs of
+ *                      consecutive shot ranges (one per rank) concatenate to the one run. */
 typedef struct lqcs_sim_options {
     uint64_t seed;
     int32_t has_seed;
@@ -110,6 +113,7 @@ typedef struct lqcs_sim_options {
     int32_t max_resident;
     uint64_t n_channels;
     const lqcs_kraus_channel* channels;
+    uint64_t shot_offset;
 } lqcs_sim_options;
 
 typedef struct lqcs_state lqcs_state; /* opaque device-resident statevector */

@@ -63,6 +63,7 @@ class SimOptions(C.Structure):
         ("max_resident", C.c_int32),
         ("n_channels", C.c_uint64),
         ("channels", C.POINTER(KrausChannelC)),
+        ("shot_offset", C.c_uint64),
     ]
 
 

@@ -131,6 +131,7 @@ void dm_run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& ga
     seg.ensure(sizeof(double) * (scan_block_count(n) + 1));
     launch_dm_diag_scan(rho->ctx, rho->d(), n, cum.as<double>(), seg.as<double>());
     std::vector<double> u(shots);
+    if (opts && opts->shot_offset) rng.discard(opts->shot_offset);   // one uniform per shot
     for (uint64_t s = 0; s < shots; ++s) u[s] = rng_uniform(rng);
     du.ensure(sizeof(double) * shots);
     didx.ensure(sizeof(uint64_t) * shots);

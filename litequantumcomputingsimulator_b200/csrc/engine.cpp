@@ -868,6 +868,7 @@ void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates
         for (const GateDesc& g : gates)
             if (g.type == LQCS_GATE_MEASURE) src[g.clbit] = g.qubits[0];
         std::vector<double> u(shots);
+        if (opts && opts->shot_offset) rng.discard(opts->shot_offset);   // one uniform per shot
         for (uint64_t s = 0; s < shots; ++s) u[s] = rng_uniform(rng);
         std::vector<uint64_t> idx(shots);
         sample(*st, u.data(), shots, idx.data(), nullptr);
@@ -884,7 +885,8 @@ void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates
     std::vector<std::vector<std::array<cd, 4>>> chans;
     for (const Channel& c : channels) chans.emplace_back(c.begin(), c.end());
     const uint32_t resident = opts ? static_cast<uint32_t>(std::max(0, opts->max_resident)) : 0;
-    run_per_shot_batched(n, gates, shots, chans, fc, rng, resident, regs);
+    run_per_shot_batched(n, gates, shots, chans, fc, rng, resident, regs,
+                         opts ? opts->shot_offset : 0);
 }
 
 // ------------------------------------------------------------------ Hamiltonians

@@ -183,7 +183,7 @@ void expectation_terms_static(const void* d_amps, uint32_t n_qubits, const char*
 void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64_t shots,
                           const std::vector<std::vector<std::array<cd, 4>>>& channels,
                           const FusionConfig& fc, Rng& rng, uint32_t max_resident,
-                          uint64_t* regs);
+                          uint64_t* regs, uint64_t shot_offset = 0);
 
 // StatevectorSimulator::run.
 void run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& gates,

@@ -299,7 +299,7 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
 
 void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64_t shots,
                           const std::vector<Channel>& model, const FusionConfig& fc_in, Rng& rng,
-                          uint32_t max_resident, uint64_t* regs) {
+                          uint32_t max_resident, uint64_t* regs, uint64_t shot_offset) {
     const bool noisy = !model.empty();
     FusionConfig fc = fc_in;
     if (noisy) fc.fuse = false;
@@ -357,6 +357,7 @@ void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64
 
     // ---- uniforms, in the reference's consumption order
     std::vector<double> u(static_cast<size_t>(shots) * K);
+    rng.discard(shot_offset * K);   // the draws of the shots before this call's first
     for (double& v : u) v = rng_uniform(rng);
 
     // ---- channels: unitary mixtures get a per-shot branch table chosen here

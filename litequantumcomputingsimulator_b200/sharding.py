@@ -60,3 +60,34 @@ def sharded_adjoint_gradient(hamiltonian, ansatz, params: np.ndarray, group=None
     dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
     both = sharded_map(fn, p, group=group, device=dev)
     return both[:, 0], both[:, 1:]
+
+
+def gather_registers(local: np.ndarray, total: int, group=None, device=None) -> np.ndarray:
+    """All-gather each rank's slice of per-shot registers (uint64) into shot order."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    counts = [shard_bounds(total, world, r) for r in range(world)]
+    longest = max(h - l for l, h in counts)
+    dev = device if device is not None else torch.device("cpu")
+    buf = torch.zeros(longest, dtype=torch.int64, device=dev)
+    if local.size:
+        buf[: local.size] = torch.as_tensor(local.astype(np.uint64).view(np.int64), device=dev)
+    gathered = [torch.zeros_like(buf) for _ in range(world)]
+    dist.all_gather(gathered, buf, group=group)
+    parts = [gathered[r][: h - l].cpu().numpy() for r, (l, h) in enumerate(counts)]
+    return np.concatenate(parts).view(np.uint64)
+
+
+def sharded_run_registers(sim, circuit, shots: int, group=None) -> np.ndarray:
+    """Per-shot registers of `shots` shots with the shots split over ranks: rank r runs its
+    contiguous range with the seeded stream advanced past the earlier ranks' shots
+    (run_registers(shot_offset=lo)), so the gathered registers equal one process's run.
+    Trajectories (noise, mid-circuit measurement) need no exchange while they run; a
+    sampling run recomputes the state on every rank."""
+    import torch
+    import torch.distributed as dist
+    lo, hi = shard_bounds(shots, dist.get_world_size(group), dist.get_rank(group))
+    local = sim.run_registers(circuit, hi - lo, shot_offset=lo) if hi > lo else np.zeros(0, np.uint64)
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
+    return gather_registers(np.asarray(local, dtype=np.uint64), shots, group=group, device=dev)

@@ -269,8 +269,9 @@ class StatevectorSimulator:
     def name(self) -> str:
         return "statevector_simulator"
 
-    def _options(self):
+    def _options(self, shot_offset: int = 0):
         o = N.SimOptions()
+        o.shot_offset = int(shot_offset)
         o.has_seed = 0 if self.seed is None else 1
         o.seed = 0 if self.seed is None else int(self.seed) & 0xFFFFFFFFFFFFFFFF
         o.fuse_gates = int(self.fuse_gates)
@@ -300,9 +301,13 @@ class StatevectorSimulator:
                C.byref(opts), regs.ctypes.data)
         return Result(registers_to_counts(regs[:shots], circuit.num_clbits()), shots)
 
-    def run_registers(self, circuit: QuantumCircuit, shots: int = 1024) -> np.ndarray:
-        """Per-shot classical registers (clbit c -> bit c) in shot order."""
-        opts, keep = self._options()
+    def run_registers(self, circuit: QuantumCircuit, shots: int = 1024,
+                      shot_offset: int = 0) -> np.ndarray:
+        """Per-shot classical registers (clbit c -> bit c) in shot order.  With shot_offset,
+        these are shots shot_offset .. shot_offset + shots - 1 of the seeded run (the
+        uniforms of the earlier shots are skipped): consecutive ranges concatenate to one
+        run, which is how sharding.sharded_run_registers splits shots over ranks."""
+        opts, keep = self._options(shot_offset)
         arr, n, _k = circuit.c_instructions()
         regs = np.zeros(max(int(shots), 1), dtype=np.uint64)
         N.call("lqcs_run", circuit.num_qubits(), circuit.num_clbits(), arr, n, int(shots),
@@ -365,8 +370,9 @@ class DensityMatrixSimulator:
         N.call("lqcs_dm_create", circuit.num_qubits(), arr, n, C.byref(opts), C.byref(h))
         return DensityMatrix(Statevector(_handle=h), circuit.num_qubits())
 
-    def run_registers(self, circuit: QuantumCircuit, shots: int = 1024) -> np.ndarray:
-        opts, keep = self._sim._options()
+    def run_registers(self, circuit: QuantumCircuit, shots: int = 1024,
+                      shot_offset: int = 0) -> np.ndarray:
+        opts, keep = self._sim._options(shot_offset)
         arr, n, _k = circuit.c_instructions()
         regs = np.zeros(max(int(shots), 1), dtype=np.uint64)
         N.call("lqcs_dm_run", circuit.num_qubits(), circuit.num_clbits(), arr, n, int(shots),

@@ -53,7 +53,7 @@ int main(void) {
   P(lqcs_instruction, params); P(lqcs_instruction, clbit); P(lqcs_instruction, qubits);
   P(lqcs_instruction, pauli);
   printf("lqcs_sim_options %zu\\n", sizeof(lqcs_sim_options));
-  P(lqcs_sim_options, n_channels); P(lqcs_sim_options, channels);
+  P(lqcs_sim_options, n_channels); P(lqcs_sim_options, channels); P(lqcs_sim_options, shot_offset);
   printf("lqcs_kraus_channel %zu\\n", sizeof(lqcs_kraus_channel));
   printf("lqcs_parametric_circuit %zu\\n", sizeof(lqcs_parametric_circuit));
   P(lqcs_parametric_circuit, n_insts); P(lqcs_parametric_circuit, param_inst);
@@ -82,6 +82,7 @@ def test_struct_layouts_match_header(tmp_path):
     assert c["lqcs_sim_options"] == C.sizeof(N.SimOptions)
     assert c["lqcs_sim_options.n_channels"] == N.SimOptions.n_channels.offset
     assert c["lqcs_sim_options.channels"] == N.SimOptions.channels.offset
+    assert c["lqcs_sim_options.shot_offset"] == N.SimOptions.shot_offset.offset
     assert c["lqcs_kraus_channel"] == C.sizeof(N.KrausChannelC)
     assert c["lqcs_parametric_circuit"] == C.sizeof(N.ParametricCircuitC)
     assert c["lqcs_parametric_circuit.n_insts"] == N.ParametricCircuitC.n_insts.offset

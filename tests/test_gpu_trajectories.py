@@ -114,3 +114,25 @@ def test_fused_terminal_measures_any_order(ref):
     want = counts_of(ref.trajectories(full, 160, 71))
     got = counts_of(lq.StatevectorSimulator(seed=71, max_resident=40).run_registers(full, 160))
     assert got == want
+
+
+@pytest.mark.parametrize("n", [6, 12])
+def test_shot_ranges_concatenate_to_one_run(n):
+    """Shots [0, 37) and [37, 100) run separately (shot_offset) give the registers of one
+    100-shot run: what sharded_run_registers relies on (gate-by-gate driver at 6 qubits,
+    fused driver at 12; sampling and density-matrix paths too)."""
+    qc = W.brickwork(n, 4, seed=n, measure=True, noise=(0.02, 0.05, 0.2))
+    sim = lq.StatevectorSimulator(seed=123, max_resident=16)
+    full = sim.run_registers(qc, 100)
+    parts = np.concatenate([sim.run_registers(qc, 37), sim.run_registers(qc, 63, shot_offset=37)])
+    assert np.array_equal(full, parts)
+    clean = W.brickwork(n, 4, seed=n, measure=True)
+    full = sim.run_registers(clean, 100)
+    parts = np.concatenate([sim.run_registers(clean, 50, shot_offset=0),
+                            sim.run_registers(clean, 50, shot_offset=50)])
+    assert np.array_equal(full, parts)
+    dm = lq.DensityMatrixSimulator(seed=9)
+    small = W.brickwork(6, 3, seed=1, measure=True, noise=(0.02, 0.05, 0.2))
+    full = dm.run_registers(small, 80)
+    parts = np.concatenate([dm.run_registers(small, 30), dm.run_registers(small, 50, shot_offset=30)])
+    assert np.array_equal(full, parts)

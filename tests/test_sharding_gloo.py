@@ -70,3 +70,39 @@ def test_two_gloo_ranks_gather_in_order(tmp_path, n_sets):
     want = _energies(items)
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) < 1e-14
+
+
+class _ShotRangeSim:
+    """Stands in for a simulator on CPU: shot s of the seeded run has register
+    s * 2654435761 mod 2^64 (any function of the global shot index), so a rank that ignores
+    its shot_offset or a gather out of order is caught."""
+
+    def run_registers(self, circuit, shots, shot_offset=0):
+        s = np.arange(shot_offset, shot_offset + shots, dtype=np.uint64)
+        return s * np.uint64(2654435761) + np.uint64(1 << 63)
+
+
+def _shots_worker(rank, world, port, shots, out_path):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch.distributed as dist
+    from datetime import timedelta
+    from litequantumcomputingsimulator_b200.sharding import sharded_run_registers
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        regs = sharded_run_registers(_ShotRangeSim(), None, shots)
+        if rank == 0:
+            np.save(out_path, regs)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("shots", [1, 9, 64])
+def test_two_gloo_ranks_shard_trajectory_shots(tmp_path, shots):
+    out = str(tmp_path / "regs.npy")
+    mp.spawn(_shots_worker, args=(2, _free_port(), shots, out), nprocs=2, join=True)
+    got = np.load(out)
+    assert got.dtype == np.uint64
+    assert np.array_equal(got, _ShotRangeSim().run_registers(None, shots))
