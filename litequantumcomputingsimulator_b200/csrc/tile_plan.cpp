@@ -206,6 +206,114 @@ double local_op_flops(const LocalOp& o, bool x_free) {
     return 8.0 * std::ldexp(1.0, static_cast<int>(o.lt.size())) * frac;
 }
 
+// Matrix of a 2^k dense op with a one-qubit matrix applied first on its target bit j:
+// M' = M (I (x) .. u .. (x) I).  Both sides may carry selector blocks: `ms` / `us` give the
+// bit of each op's selector qubit within the merged selector set.
+static void fold_into(LocalOp& q, const LocalOp& p, uint32_t j, const std::vector<uint32_t>& sel,
+                      bool after = false) {
+    const uint32_t k = static_cast<uint32_t>(q.lt.size());
+    const uint64_t D = uint64_t{1} << k;
+    const uint32_t nsel = static_cast<uint32_t>(sel.size());
+    auto index_of = [&](const std::vector<uint32_t>& own, uint32_t sv) {
+        uint32_t idx = 0;
+        for (size_t i = 0; i < own.size(); ++i) {
+            const uint32_t pos = static_cast<uint32_t>(std::find(sel.begin(), sel.end(), own[i]) - sel.begin());
+            if ((sv >> pos) & 1) idx |= 1u << i;
+        }
+        return idx;
+    };
+    std::vector<cd> out;
+    for (uint32_t sv = 0; sv < (1u << nsel); ++sv) {
+        const cd* m = q.m.data() + static_cast<size_t>(index_of(q.sel, sv)) * D * D;
+        std::array<cd, 4> u{};
+        const uint32_t pi = index_of(p.sel, sv);
+        if (p.kind == kTileDiag) {
+            u = {p.m[2 * pi], cd{0, 0}, cd{0, 0}, p.m[2 * pi + 1]};
+        } else {
+            for (int e = 0; e < 4; ++e) u[e] = p.m[4 * pi + e];
+        }
+        for (uint64_t r = 0; r < D; ++r) {
+            for (uint64_t c = 0; c < D; ++c) {
+                cd acc{0, 0};
+                if (after) {
+                    // (U M)[r][c] = sum_x U[r_j][x] M[r with bit j = x][c]
+                    const uint64_t rj = (r >> j) & 1, r0 = r & ~(uint64_t{1} << j);
+                    for (uint64_t xj = 0; xj < 2; ++xj)
+                        acc += u[rj * 2 + xj] * m[(r0 | xj << j) * D + c];
+                } else {
+                    // (M U)[r][c] = sum_x M[r][x] U[x][c]; U acts on bit j only
+                    const uint64_t cj = (c >> j) & 1, c0 = c & ~(uint64_t{1} << j);
+                    for (uint64_t xj = 0; xj < 2; ++xj)
+                        acc += m[r * D + (c0 | xj << j)] * u[xj * 2 + cj];
+                }
+                out.push_back(acc);
+            }
+        }
+    }
+    q.m = std::move(out);
+    q.sel = sel;
+}
+
+// Peephole after inner fusion: a one-qubit dense or diagonal op (no controls) moves into the
+// next op touching its qubit — or, failing that, the previous one — when that op is a dense
+// block on it without controls (the ops in between do not touch the qubit, so they commute
+// with it): the block's matrix absorbs it at no extra cost per amplitude and one operation
+// disappears.
+static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select) {
+    std::vector<char> dead(ops.size(), 0);
+    for (size_t i = 0; i < ops.size(); ++i) {
+        LocalOp& p = ops[i];
+        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || p.variant) continue;
+        const uint32_t a = p.lt[0];
+        for (size_t j = i + 1; j < ops.size(); ++j) {
+            if (dead[j]) continue;
+            LocalOp& q = ops[j];
+            const bool touches = ((q.lmask >> a) & 1) ||
+                                 std::find(q.lt.begin(), q.lt.end(), a) != q.lt.end();
+            if (!touches) continue;
+            const auto it = std::find(q.lt.begin(), q.lt.end(), a);
+            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask && !q.variant) {
+                std::vector<uint32_t> sel = q.sel;
+                for (uint32_t s : p.sel)
+                    if (std::find(sel.begin(), sel.end(), s) == sel.end()) sel.push_back(s);
+                std::sort(sel.begin(), sel.end());
+                if (sel.size() <= max_select || (p.sel.empty() && q.sel.size() <= max_select)) {
+                    fold_into(q, p, static_cast<uint32_t>(it - q.lt.begin()), sel);
+                    dead[i] = 1;
+                }
+            }
+            break;   // only the next op on the qubit
+        }
+        if (dead[i]) continue;
+        for (size_t j = i; j-- > 0;) {
+            if (dead[j]) continue;
+            LocalOp& q = ops[j];
+            const bool touches = ((q.lmask >> a) & 1) ||
+                                 std::find(q.lt.begin(), q.lt.end(), a) != q.lt.end();
+            if (!touches) continue;
+            const auto it = std::find(q.lt.begin(), q.lt.end(), a);
+            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask && !q.variant) {
+                std::vector<uint32_t> sel = q.sel;
+                for (uint32_t s : p.sel)
+                    if (std::find(sel.begin(), sel.end(), s) == sel.end()) sel.push_back(s);
+                std::sort(sel.begin(), sel.end());
+                if (sel.size() <= max_select || (p.sel.empty() && q.sel.size() <= max_select)) {
+                    fold_into(q, p, static_cast<uint32_t>(it - q.lt.begin()), sel, true);
+                    dead[i] = 1;
+                }
+            }
+            break;   // only the previous op on the qubit
+        }
+    }
+    size_t w = 0;
+    for (size_t i = 0; i < ops.size(); ++i) {
+        if (dead[i]) continue;
+        if (w != i) ops[w] = std::move(ops[i]);
+        ++w;
+    }
+    ops.resize(w);
+}
+
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
                                     const TileConfig& cfg, uint32_t max_select,
                                     const std::vector<std::array<cd, 4>>* slot_mats) {
@@ -376,6 +484,7 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
         open.push_back(std::move(nb));
     }
     for (Open& b : open) emit_block(b);
+    fold_single_qubit_ops(out, max_select);
     return out;
 }
 
