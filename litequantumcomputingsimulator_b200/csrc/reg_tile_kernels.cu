@@ -297,6 +297,9 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
     double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
     for (uint64_t tid = blockIdx.x; tid < p.n_tiles; tid += gridDim.x) {
+        // a warp's shared-memory slots differ between layouts with different warp bits:
+        // the previous tile's last remap must be done before this tile's first
+        if (p.sync_tiles) __syncthreads();
         uint64_t base = tid << p.L;
         for (uint32_t i = 0; i < p.h; ++i) base = insert_zero_bit(base, shbits[i]);
         double2 v[kE];
@@ -339,7 +342,9 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                              ((u & 8) ? r3 : 0)] = v[u];
                 }
                 cur = op.code;
-                __syncthreads();
+                const bool local = op.k != 0;   // uniform: warp bits unchanged
+                if (local) __syncwarp();
+                else __syncthreads();
                 {
                     const RegLayout& ly = slay[cur];
                     const uint32_t ts = thread_slot(ly, kTB);
@@ -349,7 +354,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                         v[u] = tile[ts ^ ((u & 1) ? r0 : 0) ^ ((u & 2) ? r1 : 0) ^
                                     ((u & 4) ? r2 : 0) ^ ((u & 8) ? r3 : 0)];
                 }
-                __syncthreads();
+                if (local) __syncwarp();
+                else __syncthreads();
                 continue;
             }
             const uint32_t tc = op.tcmask;

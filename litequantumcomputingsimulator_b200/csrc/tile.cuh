@@ -99,7 +99,7 @@ struct RegOp {
     uint32_t mat_off;         // double2 offset in the pass's staged matrices
     uint8_t kind;
     uint8_t code;             // dense / swap: register target mask; remap: new layout index
-    uint8_t k;                // dense / diag: number of targets
+    uint8_t k;                // dense / diag: number of targets; remap: 1 = warp-local
     uint8_t rcmask;           // register-index bits that must be 1 (controls, phase bits)
     uint16_t tcmask;          // thread-index bits that must be 1
     uint8_t loc[4];           // diag: target j at register bit loc, or thread bit loc & 0x7f
@@ -115,6 +115,7 @@ struct RegPass {
     uint32_t m, L, h;
     uint32_t n_ops, n_layouts, n_mat;
     uint32_t mat_stride;      // double2 between the matrices of consecutive states (0: shared)
+    uint32_t sync_tiles;      // some remap changes the warp bits: barrier between tiles
     uint32_t hbits[kTileMaxHigh];
 };
 

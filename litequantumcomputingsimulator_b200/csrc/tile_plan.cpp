@@ -591,18 +591,25 @@ size_t covered(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pen
     return c;
 }
 
-// Layout of register set S on an m-bit tile.  Thread bits ascending, except that when the
-// low five are not tile bits 0..4 the first three are picked with distinct residues mod 3:
-// tile_swizzle sends 1 << b to slot bit (b mod 3), so then the 8 lanes of a quarter warp hit
-// 8 different 16-byte bank groups in a remap.
-RegLayout make_layout(uint32_t S, uint32_t m) {
+// Layout of register set S and warp bits W on an m-bit tile.  Thread-index bits 0..4 (the
+// lanes) take the tile bits outside S and W, bits 5.. (the warps) take W in ascending order.
+// Lanes ascending, except that when they are not tile bits 0..4 the first three are picked
+// with distinct residues mod 3: tile_swizzle sends 1 << b to slot bit (b mod 3), so then the
+// 8 lanes of a quarter warp hit 8 different 16-byte bank groups in a remap.  A remap that
+// keeps W keeps every warp on the same tile indices, hence on its own shared-memory slots:
+// it needs only a warp-level barrier.
+RegLayout make_layout(uint32_t S, uint32_t W, uint32_t m) {
     RegLayout ly{};
-    std::vector<uint32_t> rb, tb;
-    for (uint32_t b = 0; b < m; ++b) ((S >> b) & 1 ? rb : tb).push_back(b);
-    if ((S & ((1u << kLaneBits) - 1u)) != 0) {
+    std::vector<uint32_t> rb, lanes, warps;
+    for (uint32_t b = 0; b < m; ++b) {
+        if ((S >> b) & 1) rb.push_back(b);
+        else if ((W >> b) & 1) warps.push_back(b);
+        else lanes.push_back(b);
+    }
+    if (lanes.size() >= 3 && lanes[0] + lanes.size() - 1 != lanes.back()) {
         std::vector<uint32_t> first, rest;
         uint32_t seen = 0;
-        for (uint32_t b : tb) {
+        for (uint32_t b : lanes) {
             if (first.size() < 3 && !((seen >> (b % 3)) & 1)) {
                 first.push_back(b);
                 seen |= 1u << (b % 3);
@@ -610,9 +617,11 @@ RegLayout make_layout(uint32_t S, uint32_t m) {
                 rest.push_back(b);
             }
         }
-        tb = first;
-        tb.insert(tb.end(), rest.begin(), rest.end());
+        lanes = first;
+        lanes.insert(lanes.end(), rest.begin(), rest.end());
     }
+    std::vector<uint32_t> tb = lanes;
+    tb.insert(tb.end(), warps.begin(), warps.end());
     for (uint32_t i = 0; i < kRegBits; ++i) {
         ly.rpos[i] = static_cast<uint8_t>(rb[i]);
         ly.rsw[i] = static_cast<uint16_t>(tile_swizzle(1u << rb[i]));
@@ -622,6 +631,26 @@ RegLayout make_layout(uint32_t S, uint32_t m) {
         ly.tsw[i] = static_cast<uint16_t>(tile_swizzle(1u << tb[i]));
     }
     return ly;
+}
+
+// `count` warp bits out of `avail`: the tile bits the pending dense operations target least
+// (ties: the higher bit), so that few later operations need a bit that is a warp bit.
+uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pending,
+                        uint32_t avail, uint32_t count) {
+    uint32_t usage[32] = {};
+    for (uint32_t i : pending)
+        if (ops[i].kind == kTileDense)
+            for (uint32_t b : ops[i].lt) ++usage[b];
+    uint32_t W = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        int best = -1;
+        for (int b = 31; b >= 0; --b) {
+            if (!((avail >> b) & 1) || ((W >> b) & 1)) continue;
+            if (best < 0 || usage[b] < usage[best]) best = b;
+        }
+        if (best >= 0) W |= 1u << best;
+    }
+    return W;
 }
 
 // Register sets of size kRegBits inside `allowed` that contain `must`, best first by
@@ -745,34 +774,57 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     for (const LocalOp& o : ops) use.push_back(op_use(o));
 
     std::vector<RegLayout> lays;
-    std::vector<uint32_t> lay_sets;
-    auto layout_index = [&](uint32_t S) {
+    std::vector<uint32_t> lay_sets, lay_warps;
+    auto layout_index = [&](uint32_t S, uint32_t W) {
         for (size_t i = 0; i < lay_sets.size(); ++i)
-            if (lay_sets[i] == S) return static_cast<uint32_t>(i);
+            if (lay_sets[i] == S && lay_warps[i] == W) return static_cast<uint32_t>(i);
         lay_sets.push_back(S);
-        lays.push_back(make_layout(S, m));
+        lay_warps.push_back(W);
+        lays.push_back(make_layout(S, W, m));
         return static_cast<uint32_t>(lay_sets.size() - 1);
     };
-    // schedule: (op, layout) in application order, remaps as (-1, new layout)
+    // schedule: (op, layout) in application order, remaps as (-1 warp-local / -2 CTA-wide,
+    // new layout)
     std::vector<std::pair<int, uint32_t>> seq;
     const uint32_t all = (1u << m) - 1u;
-    const uint32_t high = all & ~((1u << kLaneBits) - 1u);
+    const uint32_t lanes = (1u << kLaneBits) - 1u;
+    const uint32_t high = all & ~lanes;
+    const uint32_t nwarp = m - kRegBits - kLaneBits;
     std::vector<uint32_t> pending(ops.size());
     for (uint32_t i = 0; i < ops.size(); ++i) pending[i] = i;
     // the first layout loads the tile: lanes on tile bits 0..4 keep the loads coalesced
     uint32_t S = choose_set(ops, use, pending, 0, high, m);
-    uint32_t cur = layout_index(S);
+    uint32_t W = pick_warp_bits(ops, pending, high & ~S, nwarp);
+    uint32_t cur = layout_index(S, W);
+    bool sync_tiles = false;
     while (true) {
         std::vector<uint32_t> applied;
         scan(ops, use, pending, S, &applied);
         for (uint32_t i : applied) seq.emplace_back(static_cast<int>(i), cur);
         if (pending.empty()) break;
-        S = choose_set(ops, use, pending, target_mask(ops[pending.front()]), all, m);
-        cur = layout_index(S);
-        seq.emplace_back(-1, cur);
+        const uint32_t must = target_mask(ops[pending.front()]);
+        if ((must & W) == 0) {   // warp-local: the warp bits stay
+            S = choose_set(ops, use, pending, must, all & ~W, m);
+            cur = layout_index(S, W);
+            seq.emplace_back(-1, cur);
+        } else {                 // a target is a warp bit: new warp bits, CTA-wide remap
+            S = choose_set(ops, use, pending, must, all, m);
+            W = pick_warp_bits(ops, pending, all & ~S, nwarp);
+            cur = layout_index(S, W);
+            seq.emplace_back(-2, cur);
+            sync_tiles = true;
+        }
     }
-    if ((S & ((1u << kLaneBits) - 1u)) != 0)   // the store wants lanes on tile bits 0..4 again
-        seq.emplace_back(-1, layout_index(all & ~((1u << (m - kRegBits)) - 1u)));
+    if (((S | W) & lanes) != 0) {   // the store wants lanes on tile bits 0..4 again
+        if ((W & lanes) == 0) {
+            seq.emplace_back(-1, layout_index(high & ~W, W));
+        } else {
+            const uint32_t Sf = all & ~((1u << (m - kRegBits)) - 1u);
+            W = pick_warp_bits(ops, pending, high & ~Sf, nwarp);
+            seq.emplace_back(-2, layout_index(Sf, W));
+            sync_tiles = true;
+        }
+    }
 
     // records and the first state's matrices
     std::vector<RegOp> rec;
@@ -782,6 +834,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             RegOp r{};
             r.kind = kRegRemap;
             r.code = static_cast<uint8_t>(l);
+            r.k = i == -1 ? 1 : 0;   // 1: warp-local
             rec.push_back(r);
             continue;
         }
@@ -813,6 +866,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     pass.n_layouts = static_cast<uint32_t>(lays.size());
     pass.n_mat = static_cast<uint32_t>(n_mat);
     pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
+    pass.sync_tiles = sync_tiles ? 1u : 0u;
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());
     layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());
     mats_out.insert(mats_out.end(), mats.begin(), mats.end());
