@@ -67,13 +67,21 @@ def parameter_shift_gradient(hamiltonian, ansatz: ParametricCircuit, params) -> 
     return grad[: params.size].tolist()
 
 
+def _parameter_sets(params, n_params: int):
+    """params as (B, P) float64 and whether a single (P,) set was given; an ansatz without
+    parameters takes (0,) for one set or (B, 0) for B sets."""
+    p = np.asarray(params, dtype=np.float64)
+    single = p.ndim <= 1
+    if n_params == 0:
+        sets = 1 if single else p.shape[0]
+        return np.zeros((sets, 0)), single
+    return np.ascontiguousarray(p.reshape(-1, n_params)), single
+
+
 def adjoint_gradient(hamiltonian, ansatz: ParametricCircuit, params, max_resident: int = 0):
     """Batched adjoint-state gradients.  params: (P,) or (B, P).  Returns
     (energies (B,), gradients (B, P)) as numpy arrays (squeezed for a single set)."""
-    p = np.asarray(params, dtype=np.float64)
-    single = p.ndim == 1
-    p = np.ascontiguousarray(p.reshape(-1, ansatz.num_parameters()) if ansatz.num_parameters()
-                             else p.reshape(-1, 0))
+    p, single = _parameter_sets(params, ansatz.num_parameters())
     if p.shape[1] != ansatz.num_parameters():
         raise ValueError("adjoint_gradient: params size must equal num_parameters")
     b = p.shape[0]
@@ -89,7 +97,8 @@ def adjoint_gradient(hamiltonian, ansatz: ParametricCircuit, params, max_residen
 
 
 def batched_energy(hamiltonian, ansatz: ParametricCircuit, params, max_resident: int = 0):
-    p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1, ansatz.num_parameters()))
+    """Energies of B parameter sets (the forward pass of adjoint_gradient)."""
+    p, _ = _parameter_sets(params, ansatz.num_parameters())
     h, keep_h = _hamiltonian(hamiltonian)
     pc, keep_p = ansatz.c_struct()
     energies = np.zeros(p.shape[0])

@@ -49,7 +49,8 @@ def sharded_adjoint_gradient(hamiltonian, ansatz, params: np.ndarray, group=None
     (energies (B,), gradients (B, P)) on every rank."""
     import torch
     from .algorithms import adjoint_gradient
-    p = np.asarray(params, dtype=np.float64).reshape(-1, ansatz.num_parameters())
+    from .algorithms import _parameter_sets
+    p, _ = _parameter_sets(params, ansatz.num_parameters())
 
     def fn(chunk):
         if chunk.shape[0] == 0:

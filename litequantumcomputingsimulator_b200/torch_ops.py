@@ -20,8 +20,8 @@ class AdjointExpectation(torch.autograd.Function):
                 max_resident: int = 0):
         p = params.detach().to("cpu", torch.float64).numpy()
         single = p.ndim == 1
-        e, g = adjoint_gradient(hamiltonian, ansatz, p.reshape(-1, ansatz.num_parameters()),
-                                max_resident=max_resident)
+        sets = p.reshape(1, -1) if single else p   # (B, P), also for P = 0
+        e, g = adjoint_gradient(hamiltonian, ansatz, sets, max_resident=max_resident)
         grad = torch.as_tensor(np.asarray(g), dtype=params.dtype, device=params.device)
         energies = torch.as_tensor(np.asarray(e), dtype=params.dtype, device=params.device)
         if single:
