@@ -396,14 +396,16 @@ def main():
                         "tflops": round(v["flops"] / (v["ms"] / 1e3) / 1e12, 2)}
                     for k, v in by_kernel.items()}})
 
+    # extra legs (sweeps, other workloads) in the one-GPU run only: a multi-GPU run holds
+    # every GPU while rank 0 works
     extras = {}
-    if not args.no_extras and rank == 0:
+    if not args.no_extras and world == 1:
         extras = run_extras(lq, W, N, n, sv, hbm_peak, args)
 
-    # ---- e2e through the public API: run_statevector + D2H of the final state
+    # ---- e2e through the public API on every rank: run_statevector + D2H of the final state
     e2e = None
-    if rank == 0 and not args.no_e2e:
-        e2e = run_e2e(lq, qc, gate_bytes, args)
+    if not args.no_e2e:
+        e2e = run_e2e(lq, qc, gate_bytes, args, dist, device, world)
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
@@ -437,7 +439,7 @@ def main():
     return 0
 
 
-def run_e2e(lq, qc, gate_bytes, args):
+def run_e2e(lq, qc, gate_bytes, args, dist=None, device=None, world=1):
     import torch
     n = qc.num_qubits()
     try:
@@ -455,13 +457,14 @@ def run_e2e(lq, qc, gate_bytes, args):
     sv.to_numpy(out=host)
     del sv
     torch.cuda.synchronize()
+    barrier(dist)
     t0 = time.perf_counter()
     for _ in range(reps):
         sv = sim.run_statevector(qc)
         sv.to_numpy(out=host)
         del sv
-    dt = (time.perf_counter() - t0) / reps
-    return {"value": gate_bytes / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+    dt = max_over_ranks((time.perf_counter() - t0) / reps, dist, device)
+    return {"value": world * gate_bytes / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(16 << n), "s_per_step": dt, "pinned": pinned,
             "path": "StatevectorSimulator.run_statevector + Statevector.to_numpy (D2H)"}
 
