@@ -606,6 +606,35 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     except Exception as ex:  # noqa: BLE001
         out["autotune_error"] = str(ex)
 
+    # uneven qubit counts: 8 problems of 10..17 qubits (100 rp gates, 100 terms, 32 parameter
+    # sets each) as one captured graph with concurrent branches, against the same problems
+    # one call after another
+    try:
+        probs = []
+        for i, nq in enumerate(range(10, 18)):
+            pc_i, _ = W.random_pauli_ansatz(nq, 100, seed=200 + i)
+            probs.append((W.random_hamiltonian(nq, 100, seed=300 + i), pc_i))
+        def sets_for(seed):
+            return [W.random_parameter_sets(pc_i.num_parameters(), 32, seed=seed + j)
+                    for j, (h_i, pc_i) in enumerate(probs)]
+        lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, sets_for(1))])
+        for (h, pc_i), s in zip(probs, sets_for(1)):
+            lq.algorithms.adjoint_gradient(h, pc_i, s)
+        torch.cuda.synchronize()
+        s2 = sets_for(2)
+        t0 = time.perf_counter()
+        lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, s2)])
+        t_m = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for (h, pc_i), s in zip(probs, s2):
+            lq.algorithms.adjoint_gradient(h, pc_i, s)
+        t_s = time.perf_counter() - t0
+        out["ragged_8x32_sets_per_s"] = 8 * 32 / t_m
+        out["ragged_sequential_sets_per_s"] = 8 * 32 / t_s
+        out["ragged_speedup"] = t_s / t_m
+    except Exception as ex:  # noqa: BLE001
+        out["ragged_error"] = str(ex)
+
     # density-matrix backend: config-3 noise on a 13-qubit brickwork, depth 20 (rho as a
     # 26-qubit device state, 1 GiB), and the 10-qubit cross-check size
     try:

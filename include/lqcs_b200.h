@@ -352,6 +352,19 @@ int lqcs_adjoint_gradient(const lqcs_parametric_circuit* pc, const lqcs_hamilton
                           const double* params, uint64_t batch, uint32_t max_resident,
                           double* energy_out, double* grad_out);
 
+/* Adjoint gradients of several problems of different qubit counts in one call: problem p
+ * has its own ansatz pcs[p], Hamiltonian hs[p] and batches[p] parameter sets params[p]
+ * (batches[p] x n_params_p); results go to energy_out[p] / grad_out[p] (either array may be
+ * NULL, or hold NULL entries).  Each problem keeps a resident batch and all problems run as
+ * one captured CUDA graph whose branches execute concurrently, replayed on later calls with
+ * the same problems (new parameter values allowed).  Problems below 5 qubits, or more than
+ * half the free device memory in total, run one after another instead.  Engine extension:
+ * no counterpart in the reference. */
+int lqcs_adjoint_gradient_multi(uint64_t n_problems, const lqcs_parametric_circuit* const* pcs,
+                                const lqcs_hamiltonian* const* hs, const double* const* params,
+                                const uint64_t* batches, double* const* energy_out,
+                                double* const* grad_out);
+
 /* Energies only, batched (forward pass of lqcs_adjoint_gradient). */
 int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
                         const double* params, uint64_t batch, uint32_t max_resident,

@@ -96,6 +96,35 @@ def adjoint_gradient(hamiltonian, ansatz: ParametricCircuit, params, max_residen
     return energies, grads
 
 
+def adjoint_gradient_multi(problems) -> list:
+    """Adjoint gradients of several problems of different qubit counts in one call.
+    problems: [(hamiltonian, ansatz, params (B, P) or (P,)), ...].  All problems run as one
+    captured CUDA graph, replayed on later calls with the same problems (new parameter values
+    allowed).  Returns [(energies (B,), gradients (B, P)), ...] in problem order."""
+    keep, pcs, hs, ps, outs_e, outs_g = [], [], [], [], [], []
+    batches = np.zeros(len(problems), dtype=np.uint64)
+    for i, (ham, ansatz, params) in enumerate(problems):
+        p, _ = _parameter_sets(params, ansatz.num_parameters())
+        h, kh = _hamiltonian(ham)
+        pc, kp = ansatz.c_struct()
+        e = np.zeros(p.shape[0])
+        g = np.zeros((p.shape[0], ansatz.num_parameters()))
+        keep += [p, h, kh, pc, kp, e, g]
+        pcs.append(C.addressof(pc))
+        hs.append(C.addressof(h))
+        ps.append(p.ctypes.data)
+        outs_e.append(e)
+        outs_g.append(g)
+        batches[i] = p.shape[0]
+    n = len(problems)
+    arr = lambda xs: (C.c_void_p * max(n, 1))(*xs)   # noqa: E731
+    a_pc, a_h, a_p = arr(pcs), arr(hs), arr(ps)
+    a_e = arr([e.ctypes.data for e in outs_e])
+    a_g = arr([g.ctypes.data if g.size else None for g in outs_g])
+    N.call("lqcs_adjoint_gradient_multi", n, a_pc, a_h, a_p, batches.ctypes.data, a_e, a_g)
+    return list(zip(outs_e, outs_g))
+
+
 def batched_energy(hamiltonian, ansatz: ParametricCircuit, params, max_resident: int = 0):
     """Energies of B parameter sets (the forward pass of adjoint_gradient)."""
     p, _ = _parameter_sets(params, ansatz.num_parameters())

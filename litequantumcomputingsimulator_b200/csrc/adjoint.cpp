@@ -242,6 +242,10 @@ std::mutex g_plan_mu;
 std::vector<std::unique_ptr<AdjointPlan>> g_plans;
 constexpr size_t kKeptPlans = 2;
 
+std::unique_ptr<AdjointPlan> build_plan(const std::vector<GateDesc>& tmpl,
+                                        const std::vector<int>& param_of, const Hamiltonian& h,
+                                        uint32_t n, uint64_t np, uint32_t R, uint64_t dkey);
+
 AdjointPlan& adjoint_plan(const std::vector<GateDesc>& tmpl, const std::vector<int>& param_of,
                           const Hamiltonian& h, uint32_t n, uint64_t np, uint64_t batch,
                           uint32_t max_resident) {
@@ -254,6 +258,15 @@ AdjointPlan& adjoint_plan(const std::vector<GateDesc>& tmpl, const std::vector<i
     std::lock_guard<std::mutex> lk(g_plan_mu);
     for (auto& p : g_plans)
         if (p->key == dkey) return *p;
+    auto plan = build_plan(tmpl, param_of, h, n, np, R, dkey);
+    if (g_plans.size() >= kKeptPlans) g_plans.erase(g_plans.begin());
+    g_plans.push_back(std::move(plan));
+    return *g_plans.back();
+}
+
+std::unique_ptr<AdjointPlan> build_plan(const std::vector<GateDesc>& tmpl,
+                                        const std::vector<int>& param_of, const Hamiltonian& h,
+                                        uint32_t n, uint64_t np, uint32_t R, uint64_t dkey) {
     auto plan = std::make_unique<AdjointPlan>();
     plan->key = dkey;
     plan->n = n;
@@ -293,9 +306,7 @@ AdjointPlan& adjoint_plan(const std::vector<GateDesc>& tmpl, const std::vector<i
     plan->d_part.ensure(sizeof(double) * 64 * R);
     plan->d_energy.ensure(sizeof(double) * R);
     plan->d_grad.ensure(sizeof(double) * std::max<uint64_t>(1, np) * R);
-    if (g_plans.size() >= kKeptPlans) g_plans.erase(g_plans.begin());
-    g_plans.push_back(std::move(plan));
-    return *g_plans.back();
+    return plan;
 }
 
 }  // namespace
@@ -402,6 +413,194 @@ void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
                           grad_out + (b0 + b) * np);
         }
     }
+}
+
+// ------------------------------------------------------------------ ragged batches
+
+namespace {
+
+// Problems of different qubit counts (each its own ansatz, Hamiltonian and parameter sets)
+// in one CUDA graph: every problem keeps its plan and stream; the capture forks from an
+// origin stream to all of them and joins back, so a call is one graph launch whose
+// branches run concurrently — small states that leave most of the GPU idle on their own
+// fill it together.
+struct MultiPlan {
+    uint64_t key = 0;
+    std::vector<std::unique_ptr<AdjointPlan>> plans;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    bool direct = false;   // capture failed: launch the branches without a graph
+
+    MultiPlan() = default;
+    MultiPlan(const MultiPlan&) = delete;
+    MultiPlan& operator=(const MultiPlan&) = delete;
+    ~MultiPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (cudaEvent_t e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        plans.clear();
+        if (origin) cudaStreamDestroy(origin);
+    }
+
+    void enqueue_all() {
+        cuda_check(cudaEventRecord(fork, origin), "cudaEventRecord");
+        for (size_t i = 0; i < plans.size(); ++i) {
+            cuda_check(cudaStreamWaitEvent(plans[i]->stream, fork, 0), "cudaStreamWaitEvent");
+            plans[i]->enqueue(plans[i]->R);
+            cuda_check(cudaEventRecord(joins[i], plans[i]->stream), "cudaEventRecord");
+            cuda_check(cudaStreamWaitEvent(origin, joins[i], 0), "cudaStreamWaitEvent");
+        }
+    }
+
+    void run() {
+        const char* e = std::getenv("LQCS_GRAPHS");
+        if (direct || (e && e[0] == '0')) {
+            enqueue_all();
+            return;
+        }
+        if (!exec) {
+            const uint64_t k0 = launch_count();
+            cudaGraph_t g = nullptr;
+            bool ok = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                try {
+                    enqueue_all();
+                } catch (...) {
+                    ok = false;
+                }
+                cudaGraph_t done = nullptr;
+                const bool ended = cudaStreamEndCapture(origin, &done) == cudaSuccess;
+                g = done;
+                ok = ok && ended && g;
+            }
+            if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            if (!ok) {
+                cudaGetLastError();
+                exec = nullptr;
+                direct = true;
+                enqueue_all();
+                return;
+            }
+            kernels = launch_count() - k0;
+            cuda_check(cudaGraphLaunch(exec, origin), "cudaGraphLaunch");
+            return;   // the capture counted this call's kernels
+        }
+        cuda_check(cudaGraphLaunch(exec, origin), "cudaGraphLaunch");
+        count_launch(kernels);
+    }
+};
+
+std::mutex g_multi_mu;
+std::vector<std::unique_ptr<MultiPlan>> g_multi;
+
+struct Problem {
+    std::vector<GateDesc> tmpl;
+    std::vector<uint64_t> pinst;
+    std::vector<int> param_of;
+    Hamiltonian h;
+    uint32_t n = 0;
+};
+
+}  // namespace
+
+void adjoint_batched_multi(uint64_t n_problems, const lqcs_parametric_circuit* const* pcs,
+                           const lqcs_hamiltonian* const* hs, const double* const* params,
+                           const uint64_t* batches, double* const* energy_out,
+                           double* const* grad_out) {
+    if (n_problems == 0) return;
+    if (!pcs || !hs || !params || !batches) invalid("adjoint_gradient_multi: null arrays");
+    std::vector<Problem> probs(n_problems);
+    double need = 0.0;
+    bool fused = true;
+    for (uint64_t p = 0; p < n_problems; ++p) {
+        if (!pcs[p]) invalid("adjoint_gradient_multi: parametric circuit is null");
+        Problem& q = probs[p];
+        check_pc(pcs[p], q.tmpl, q.pinst);
+        q.n = pcs[p]->n_qubits;
+        q.h = decode_hamiltonian(hs[p], q.n);
+        q.param_of.assign(q.tmpl.size(), -1);
+        for (uint64_t i = 0; i < q.pinst.size(); ++i) q.param_of[q.pinst[i]] = static_cast<int>(i);
+        if (batches[p] > 0 && !params[p] && !q.pinst.empty()) invalid("adjoint_gradient_multi: params is null");
+        need += 2.0 * static_cast<double>(batches[p]) * 16.0 * std::ldexp(1.0, static_cast<int>(q.n));
+        fused &= q.n >= 5 && batches[p] > 0;
+    }
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    if (!fused || need > 0.5 * static_cast<double>(free_b)) {
+        // one problem after another (each still batched)
+        for (uint64_t p = 0; p < n_problems; ++p)
+            adjoint_batched(pcs[p], probs[p].h, params[p], batches[p], 0,
+                            energy_out ? energy_out[p] : nullptr, grad_out ? grad_out[p] : nullptr);
+        return;
+    }
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::vector<uint64_t> keys(n_problems);
+    uint64_t mkey = 1469598103934665603ull ^ (static_cast<uint64_t>(dev) << 56);
+    for (uint64_t p = 0; p < n_problems; ++p) {
+        keys[p] = plan_key(probs[p].tmpl, probs[p].param_of, probs[p].h, probs[p].n,
+                           static_cast<uint32_t>(batches[p])) ^ (static_cast<uint64_t>(dev) << 56);
+        mkey = (mkey ^ keys[p]) * 1099511628211ull;
+    }
+    std::lock_guard<std::mutex> lk(g_multi_mu);
+    MultiPlan* mp = nullptr;
+    for (auto& m : g_multi)
+        if (m->key == mkey) mp = m.get();
+    if (!mp) {
+        auto m = std::make_unique<MultiPlan>();
+        m->key = mkey;
+        cuda_check(cudaStreamCreateWithFlags(&m->origin, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (uint64_t p = 0; p < n_problems; ++p) {
+            m->plans.push_back(build_plan(probs[p].tmpl, probs[p].param_of, probs[p].h, probs[p].n,
+                                          probs[p].pinst.size(), static_cast<uint32_t>(batches[p]),
+                                          keys[p]));
+            cudaEvent_t ev = nullptr;
+            cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+            m->joins.push_back(ev);
+        }
+        if (g_multi.size() >= kKeptPlans) g_multi.erase(g_multi.begin());
+        g_multi.push_back(std::move(m));
+        mp = g_multi.back().get();
+    }
+    // (cos, sin) tables of every problem, uploaded in order on the origin stream
+    std::vector<std::vector<double2>> tabs(2 * n_problems);
+    for (uint64_t p = 0; p < n_problems; ++p) {
+        const AdjointPlan& pl = *mp->plans[p];
+        const uint64_t np = pl.np, R = pl.R;
+        std::vector<double2>& cs = tabs[2 * p];
+        std::vector<double2>& csi = tabs[2 * p + 1];
+        cs.resize(np * R);
+        csi.resize(np * R);
+        for (uint64_t k = 0; k < np; ++k) {
+            for (uint64_t b = 0; b < R; ++b) {
+                const double hh = params[p][b * np + k] / 2;
+                cs[k * R + b] = make_double2(std::cos(hh), std::sin(hh));
+                csi[k * R + b] = make_double2(std::cos(hh), -std::sin(hh));
+            }
+        }
+        if (np) {
+            cuda_check(cudaMemcpyAsync(pl.d_cs.ptr, cs.data(), sizeof(double2) * np * R,
+                                       cudaMemcpyHostToDevice, mp->origin), "H2D");
+            cuda_check(cudaMemcpyAsync(pl.d_csi.ptr, csi.data(), sizeof(double2) * np * R,
+                                       cudaMemcpyHostToDevice, mp->origin), "H2D");
+        }
+    }
+    mp->run();
+    for (uint64_t p = 0; p < n_problems; ++p) {
+        const AdjointPlan& pl = *mp->plans[p];
+        if (energy_out && energy_out[p])
+            cuda_check(cudaMemcpyAsync(energy_out[p], pl.d_energy.ptr, sizeof(double) * pl.R,
+                                       cudaMemcpyDeviceToHost, mp->origin), "D2H energies");
+        if (grad_out && grad_out[p] && pl.np)
+            cuda_check(cudaMemcpyAsync(grad_out[p], pl.d_grad.ptr, sizeof(double) * pl.np * pl.R,
+                                       cudaMemcpyDeviceToHost, mp->origin), "D2H gradients");
+    }
+    cuda_check(cudaStreamSynchronize(mp->origin), "adjoint_gradient_multi");
 }
 
 }  // namespace lqcs_b200

@@ -419,6 +419,15 @@ int lqcs_adjoint_gradient(const lqcs_parametric_circuit* pc, const lqcs_hamilton
     });
 }
 
+int lqcs_adjoint_gradient_multi(uint64_t n_problems, const lqcs_parametric_circuit* const* pcs,
+                                const lqcs_hamiltonian* const* hs, const double* const* params,
+                                const uint64_t* batches, double* const* energy_out,
+                                double* const* grad_out) {
+    return guarded([&] {
+        lqcs_b200::adjoint_batched_multi(n_problems, pcs, hs, params, batches, energy_out, grad_out);
+    });
+}
+
 int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
                         const double* params, uint64_t batch, uint32_t max_resident,
                         double* energy_out) {

@@ -207,5 +207,9 @@ void parameter_shift(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
 void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
                      const double* params, uint64_t batch, uint32_t max_resident,
                      double* energy_out, double* grad_out);
+void adjoint_batched_multi(uint64_t n_problems, const lqcs_parametric_circuit* const* pcs,
+                           const lqcs_hamiltonian* const* hs, const double* const* params,
+                           const uint64_t* batches, double* const* energy_out,
+                           double* const* grad_out);
 
 }  // namespace lqcs_b200

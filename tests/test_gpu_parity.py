@@ -360,3 +360,34 @@ def test_adjoint_graph_replay_new_parameters(ref, monkeypatch):
         want = ref.parameter_shift_gradient(h, pc, sets2[b])
         assert np.max(np.abs(g2[b] - want)) < 1e-9
     assert not np.allclose(g1, g2)
+
+
+def test_adjoint_multi_ragged_problems(ref, monkeypatch):
+    """Problems of 6, 9, 12 and 14 qubits (own ansatz, Hamiltonian and batch each) in one
+    call — one captured graph, concurrent branches — equal the one-problem calls bit for
+    bit, on the capture and on a replay with new parameters; small problems fall back to
+    one-by-one and agree too."""
+    probs = []
+    for i, (n, b) in enumerate([(6, 3), (9, 5), (12, 2), (14, 4)]):
+        pc, _ = W.random_pauli_ansatz(n, 10 + 3 * i, seed=50 + i, max_w=min(8, n))
+        h = W.random_hamiltonian(n, 20 + i, seed=60 + i)
+        probs.append((h, pc, b))
+    for seed in (70, 71):   # capture, then replay
+        sets = [W.random_parameter_sets(pc.num_parameters(), b, seed=seed + j)
+                for j, (h, pc, b) in enumerate(probs)]
+        got = lq.algorithms.adjoint_gradient_multi([(h, pc, s) for (h, pc, b), s in zip(probs, sets)])
+        for (h, pc, b), s, (e, g) in zip(probs, sets, got):
+            e1, g1 = lq.algorithms.adjoint_gradient(h, pc, s)
+            assert np.array_equal(e, e1) and np.array_equal(g, g1)
+    want = ref.parameter_shift_gradient(probs[1][0], probs[1][1], sets[1][2])
+    assert np.max(np.abs(got[1][1][2] - want)) < 1e-9
+    monkeypatch.setenv("LQCS_GRAPHS", "0")
+    direct = lq.algorithms.adjoint_gradient_multi([(h, pc, s) for (h, pc, b), s in zip(probs, sets)])
+    for (e, g), (e2, g2) in zip(got, direct):
+        assert np.array_equal(e, e2) and np.array_equal(g, g2)
+    small, _ = W.random_pauli_ansatz(3, 6, seed=9, max_w=3)
+    hs = W.random_hamiltonian(3, 5, seed=8)
+    ss = W.random_parameter_sets(small.num_parameters(), 2, seed=7)
+    (e, g), _ = lq.algorithms.adjoint_gradient_multi([(hs, small, ss), probs[0][:2] + (sets[0],)])
+    e1, g1 = lq.algorithms.adjoint_gradient(hs, small, ss)
+    assert np.max(np.abs(g - g1)) < 1e-12 and np.max(np.abs(e - e1)) < 1e-12
