@@ -160,6 +160,7 @@ SIGNATURES = {
                                         C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p]),
     "lqcs_adjoint_gradient_multi": (C.c_int, [C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
+    "lqcs_release_caches": (C.c_int, []),
     "lqcs_batched_energy": (C.c_int, [_P(ParametricCircuitC), _P(HamiltonianC), C.c_void_p,
                                       C.c_uint64, C.c_uint32, C.c_void_p]),
     "lqcs_fusion_plan": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32, C.c_int32,

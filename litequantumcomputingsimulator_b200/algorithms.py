@@ -125,6 +125,12 @@ def adjoint_gradient_multi(problems) -> list:
     return list(zip(outs_e, outs_g))
 
 
+def release_caches() -> None:
+    """Free the device memory kept between gradient calls (cached plans and graphs) and the
+    autotuner's remembered choices."""
+    N.call("lqcs_release_caches")
+
+
 def batched_energy(hamiltonian, ansatz: ParametricCircuit, params, max_resident: int = 0):
     """Energies of B parameter sets (the forward pass of adjoint_gradient)."""
     p, _ = _parameter_sets(params, ansatz.num_parameters())

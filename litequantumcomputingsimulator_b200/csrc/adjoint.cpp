@@ -603,4 +603,13 @@ void adjoint_batched_multi(uint64_t n_problems, const lqcs_parametric_circuit* c
     cuda_check(cudaStreamSynchronize(mp->origin), "adjoint_gradient_multi");
 }
 
+void release_adjoint_plans() {
+    {
+        std::lock_guard<std::mutex> lk(g_multi_mu);
+        g_multi.clear();
+    }
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans.clear();
+}
+
 }  // namespace lqcs_b200

@@ -428,6 +428,13 @@ int lqcs_adjoint_gradient_multi(uint64_t n_problems, const lqcs_parametric_circu
     });
 }
 
+int lqcs_release_caches(void) {
+    return guarded([&] {
+        lqcs_b200::release_adjoint_plans();
+        lqcs_b200::clear_autotune_cache();
+    });
+}
+
 int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
                         const double* params, uint64_t batch, uint32_t max_resident,
                         double* energy_out) {

@@ -434,6 +434,11 @@ static uint64_t circuit_key(const std::vector<GateDesc>& gates, uint32_t n) {
 static std::mutex g_tune_mu;
 static std::map<uint64_t, TuneCandidate> g_tuned;
 
+void clear_autotune_cache() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned.clear();
+}
+
 std::vector<TuneTiming> autotune(const std::vector<GateDesc>& gates, uint32_t n, size_t* best) {
     std::vector<TuneTiming> out;
     size_t free_b = 0, total_b = 0;

@@ -97,6 +97,7 @@ struct TuneTiming {
 // n-qubit state and remembers the fastest for this circuit; fusion_mode 5 compiles with it.
 // Empty when no scratch state fits in device memory (mode 5 then uses the default plan).
 std::vector<TuneTiming> autotune(const std::vector<GateDesc>& gates, uint32_t n, size_t* best);
+void clear_autotune_cache();
 uint32_t default_fusion_width();
 
 // Compile a list of unitary gates to a Program (fused or gate by gate).
@@ -207,6 +208,8 @@ void parameter_shift(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
 void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
                      const double* params, uint64_t batch, uint32_t max_resident,
                      double* energy_out, double* grad_out);
+// Frees the cached adjoint plans (their resident state batches and graphs).
+void release_adjoint_plans();
 void adjoint_batched_multi(uint64_t n_problems, const lqcs_parametric_circuit* const* pcs,
                            const lqcs_hamiltonian* const* hs, const double* const* params,
                            const uint64_t* batches, double* const* energy_out,

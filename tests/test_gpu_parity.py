@@ -391,3 +391,19 @@ def test_adjoint_multi_ragged_problems(ref, monkeypatch):
     (e, g), _ = lq.algorithms.adjoint_gradient_multi([(hs, small, ss), probs[0][:2] + (sets[0],)])
     e1, g1 = lq.algorithms.adjoint_gradient(hs, small, ss)
     assert np.max(np.abs(g - g1)) < 1e-12 and np.max(np.abs(e - e1)) < 1e-12
+
+
+def test_release_caches_frees_plan_memory(ref):
+    import torch
+    pc, _ = W.random_pauli_ansatz(16, 20, seed=3)
+    h = W.random_hamiltonian(16, 10, seed=4)
+    sets = W.random_parameter_sets(pc.num_parameters(), 64, seed=5)
+    lq.algorithms.release_caches()
+    free0 = torch.cuda.mem_get_info()[0]
+    e1, g1 = lq.algorithms.adjoint_gradient(h, pc, sets)
+    held = free0 - torch.cuda.mem_get_info()[0]
+    assert held >= 2 * 64 * (16 << 16)           # two resident batches of 64 states
+    lq.algorithms.release_caches()
+    assert torch.cuda.mem_get_info()[0] - free0 > -(16 << 20)
+    e2, g2 = lq.algorithms.adjoint_gradient(h, pc, sets)   # rebuilt after the release
+    assert np.array_equal(e1, e2) and np.array_equal(g1, g2)
