@@ -220,6 +220,25 @@ __device__ __forceinline__ void dispatch_swapx(double2 (&v)[kE], uint32_t code, 
     }
 }
 
+// Diagonal whose entry bits sit on register-index bits R (and on thread bits, fixed per
+// thread in tpart): amplitude u takes entry tpart | e(u & R), so a thread loads each of its
+// 2^|R| distinct entries once and multiplies the 16 / 2^|R| amplitudes that share it.
+template <int R>
+__device__ __forceinline__ void reg_diag_r(double2 (&v)[kE], uint32_t mat, uint32_t rcmask,
+                                           uint32_t tpart, uint32_t rb0, uint32_t rb1,
+                                           uint32_t rb2, uint32_t rb3) {
+#pragma unroll
+    for (int pt = 0; pt < kE; ++pt) {
+        if ((pt & R) != pt) continue;
+        const uint32_t e = tpart | ((pt & 1) ? rb0 : 0u) | ((pt & 2) ? rb1 : 0u) |
+                           ((pt & 4) ? rb2 : 0u) | ((pt & 8) ? rb3 : 0u);
+        const double2 f = lds2(mat + 16u * e);
+#pragma unroll
+        for (int u = 0; u < kE; ++u)
+            if ((u & R) == pt && (u & rcmask) == rcmask) v[u] = cmul(f, v[u]);
+    }
+}
+
 // Entry (tpart | bits picked from u) of a diagonal for every amplitude u.
 __device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, uint32_t mat,
                                          uint32_t rcmask) {
@@ -236,12 +255,16 @@ __device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, uint
             rb3 |= loc == 3 ? bit : 0u;
         }
     }
-#pragma unroll
-    for (int u = 0; u < kE; ++u) {
-        if ((u & rcmask) != rcmask) continue;
-        const uint32_t e = tpart | ((u & 1) ? rb0 : 0u) | ((u & 2) ? rb1 : 0u) |
-                           ((u & 4) ? rb2 : 0u) | ((u & 8) ? rb3 : 0u);
-        v[u] = cmul(lds2(mat + 16u * e), v[u]);
+    const uint32_t R = (rb0 ? 1u : 0u) | (rb1 ? 2u : 0u) | (rb2 ? 4u : 0u) | (rb3 ? 8u : 0u);
+    switch (R) {
+#define LQCS_DIAG_CASE(r) \
+    case r: reg_diag_r<r>(v, mat, rcmask, tpart, rb0, rb1, rb2, rb3); break;
+        LQCS_DIAG_CASE(0) LQCS_DIAG_CASE(1) LQCS_DIAG_CASE(2) LQCS_DIAG_CASE(3)
+        LQCS_DIAG_CASE(4) LQCS_DIAG_CASE(5) LQCS_DIAG_CASE(6) LQCS_DIAG_CASE(7)
+        LQCS_DIAG_CASE(8) LQCS_DIAG_CASE(9) LQCS_DIAG_CASE(10) LQCS_DIAG_CASE(11)
+        LQCS_DIAG_CASE(12) LQCS_DIAG_CASE(13) LQCS_DIAG_CASE(14)
+        default: reg_diag_r<15>(v, mat, rcmask, tpart, rb0, rb1, rb2, rb3); break;
+#undef LQCS_DIAG_CASE
     }
 }
 
@@ -272,11 +295,17 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     double2* smat = tile + (1u << M);
     RegOp* sops = reinterpret_cast<RegOp*>(smat + p.n_mat);
     RegLayout* slay = reinterpret_cast<RegLayout*>(sops + p.n_ops);
+    // per-tile diagonal tables, two sets (tile parity) on a 16-byte boundary
+    double2* sdyn = reinterpret_cast<double2*>(
+        (reinterpret_cast<uintptr_t>(slay + p.n_layouts) + 15u) & ~uintptr_t{15});
     __shared__ uint64_t gbit[kRegMaxBits];   // global offset of each tile bit
     __shared__ uint32_t shbits[kTileMaxHigh];
+    __shared__ uint32_t sdynrec[kRegMaxDyn];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (uint32_t i = 0; i < kTileMaxHigh; ++i) shbits[i] = p.hbits[i];   // static indices
+#pragma unroll
+        for (uint32_t i = 0; i < kRegMaxDyn; ++i) sdynrec[i] = p.dyn_rec[i];
         for (uint32_t b = 0; b < M; ++b)
             gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
     }
@@ -295,8 +324,10 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     }
     __syncthreads();
     const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
+    const uint32_t sdyn_addr = static_cast<uint32_t>(__cvta_generic_to_shared(sdyn));
     double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
-    for (uint64_t tid = blockIdx.x; tid < p.n_tiles; tid += gridDim.x) {
+    uint32_t parity = 0;
+    for (uint64_t tid = blockIdx.x; tid < p.n_tiles; tid += gridDim.x, parity ^= 1u) {
         // a warp's shared-memory slots differ between layouts with different warp bits:
         // the previous tile's last remap must be done before this tile's first
         if (p.sync_tiles) __syncthreads();
@@ -325,6 +356,30 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             const double2* row = s + nb;
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(16u << p.L)
                          : "memory");
+        }
+        // Per-tile diagonals: entry e of table d is its base entry times every gated term
+        // whose out-of-tile qubits are all 1 in this tile and whose entry bits e contains.
+        // The barrier after the build also ends the use of the other parity's tables (every
+        // warp has finished the previous tile), so the next tile may overwrite them.
+        const uint32_t dyn_base = parity * p.dyn_entries;
+        if (p.n_dyn) {
+            for (uint32_t w = threadIdx.x; w < p.n_dyn * 64u; w += kT) {
+                const RegOp& op = sops[sdynrec[w >> 6]];
+                const uint32_t e = w & 63u;
+                if (e >= (1u << op.k)) continue;
+                const double2* src = smat + op.mat_off;
+                double2 acc = src[e];
+                const double2* term = src + (1u << op.k);
+                for (uint32_t t = 0; t < op.nterm; ++t) {
+                    const double2 meta = term[2 * t + 1];
+                    const uint64_t hi = static_cast<uint64_t>(meta.y);
+                    const uint64_t gc = static_cast<uint64_t>(meta.x) | ((hi >> 6) << 32);
+                    const uint32_t em = static_cast<uint32_t>(hi & 63u);
+                    if ((base & gc) == gc && (e & em) == em) acc = cmul(term[2 * t], acc);
+                }
+                sdyn[dyn_base + op.dyn_off + e] = acc;
+            }
+            __syncthreads();
         }
         uint32_t cur = 0;
         for (uint32_t o = 0; o < p.n_ops; ++o) {
@@ -369,7 +424,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                 const uint32_t k2 = kind == kRegDense ? 2u * op.k : op.k;
                 moff += sel << k2;
             }
-            const uint32_t mat = smat_addr + 16u * moff;
+            const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
+                                                     : smat_addr + 16u * moff;
             if (kind == kRegDense) {
                 dispatch_dense(v, op.code, mat, rc);
             } else if (kind == kRegPhase) {
@@ -439,8 +495,10 @@ void launch_m(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& 
 }  // namespace
 
 size_t reg_smem_bytes(const RegPass& pass) {
-    return sizeof(double2) * ((size_t{1} << pass.m) + pass.n_mat) + sizeof(RegOp) * pass.n_ops +
-           sizeof(RegLayout) * pass.n_layouts;
+    const size_t records = sizeof(double2) * ((size_t{1} << pass.m) + pass.n_mat) +
+                           sizeof(RegOp) * pass.n_ops + sizeof(RegLayout) * pass.n_layouts;
+    return pass.n_dyn ? ((records + 15) & ~size_t{15}) + sizeof(double2) * 2 * pass.dyn_entries
+                      : records;
 }
 
 void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
@@ -451,7 +509,8 @@ void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t bat
     p.n_tiles = (uint64_t{1} << n) >> p.m;
     const size_t smem = reg_smem_bytes(p);
     if (smem > kTileMaxSmem || p.m < kRegMinBits || p.m > kRegMaxBits || p.h > kTileMaxHigh ||
-        p.n_layouts < 1 || p.n_ops > kRegMaxRecords || p.n_mat > kRegMaxMatrix)
+        p.n_layouts < 1 || p.n_ops > kRegMaxRecords || p.n_mat > kRegMaxMatrix ||
+        p.n_dyn > kRegMaxDyn || p.dyn_entries > kRegMaxDynEntries)
         throw std::logic_error("register tile pass: unsupported shape");
     switch (p.m) {
         case 9: launch_m<9>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats); break;

@@ -83,8 +83,16 @@ constexpr uint32_t kRegMaxRecords = 256;        // operations + remaps per pass
 constexpr uint32_t kRegMaxLayouts = 128;
 constexpr uint32_t kRegMaxMatrix = 2048;        // double2 of matrices staged per pass (32 KiB)
 constexpr uint32_t kRegMaxSelect = 2;           // out-of-tile selector qubits per operation
+constexpr uint32_t kRegMaxDiag = 6;             // widest diagonal operation (64 entries)
+constexpr uint32_t kRegMaxDyn = 8;              // per-tile diagonals per pass
+constexpr uint32_t kRegMaxDynEntries = 512;     // their table entries per pass
+constexpr uint32_t kRegMaxDynTerms = 48;        // gated phase terms of one per-tile diagonal
 
-enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4 };
+// kRegDiagDyn: a diagonal whose table is built at the start of every tile from a base table
+// and gated phase terms (the matrices hold the 2^k base entries, then per term its factor and
+// a word pair {out-of-tile mask, entry mask}); it is applied like kRegDiag.
+enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4,
+                 kRegDiagDyn = 5 };
 
 struct RegLayout {
     uint16_t rsw[kRegBits];   // tile_swizzle(1 << rpos[i])
@@ -102,11 +110,13 @@ struct RegOp {
     uint8_t k;                // dense / diag: number of targets; remap: 1 = warp-local
     uint8_t rcmask;           // register-index bits that must be 1 (controls, phase bits)
     uint16_t tcmask;          // thread-index bits that must be 1
-    uint8_t loc[4];           // diag: target j at register bit loc, or thread bit loc & 0x7f
+    uint8_t loc[kRegMaxDiag]; // diag: target j at register bit loc, or thread bit loc & 0x7f
                               // when loc & 0x80
     uint8_t nsel;             // dense / diag: the tile's bits at qubits selq[0..nsel) pick
     uint8_t selq[kRegMaxSelect];   // one of 2^nsel consecutive matrices
-    uint8_t pad[7];
+    uint8_t nterm;            // per-tile diagonal: gated phase terms
+    uint16_t dyn_off;         // per-tile diagonal: first entry in the per-tile tables
+    uint8_t pad[2];
 };
 
 struct RegPass {
@@ -117,6 +127,9 @@ struct RegPass {
     uint32_t mat_stride;      // double2 between the matrices of consecutive states (0: shared)
     uint32_t sync_tiles;      // some remap changes the warp bits: barrier between tiles
     uint32_t hbits[kTileMaxHigh];
+    uint32_t n_dyn;           // per-tile diagonals: their record indices and table entries
+    uint32_t dyn_entries;
+    uint8_t dyn_rec[kRegMaxDyn];
 };
 
 static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");

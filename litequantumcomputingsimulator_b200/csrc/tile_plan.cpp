@@ -254,6 +254,151 @@ static void fold_into(LocalOp& q, const LocalOp& p, uint32_t j, const std::vecto
     q.sel = sel;
 }
 
+// Diagonal form of a phase or diagonal op without local controls: local bits (ascending)
+// and the 2^k entries.  A phase multiplies where all its bits are 1.
+static bool diagonal_form(const LocalOp& o, std::vector<uint32_t>& bits, std::vector<cd>& d) {
+    if (o.variant || !o.sel.empty() || !o.dyn.empty()) return false;
+    if (o.kind == kTilePhase) {
+        bits.clear();
+        for (uint32_t b = 0; b < 32; ++b)
+            if ((o.lmask >> b) & 1) bits.push_back(b);
+        d.assign(size_t{1} << bits.size(), cd{1, 0});
+        d.back() = o.m[0];
+        return true;
+    }
+    if (o.kind != kTileDiag || o.lmask) return false;
+    // entries in local order (bit j <-> lt[j]); re-index to ascending bits
+    std::vector<uint32_t> order(o.lt.size());
+    for (size_t j = 0; j < order.size(); ++j) order[j] = static_cast<uint32_t>(j);
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return o.lt[a] < o.lt[b]; });
+    bits.clear();
+    for (uint32_t j : order) bits.push_back(o.lt[j]);
+    const size_t D = size_t{1} << bits.size();
+    d.assign(D, cd{1, 0});
+    for (size_t e = 0; e < D; ++e) {
+        size_t src = 0;
+        for (size_t q = 0; q < order.size(); ++q)
+            if ((e >> q) & 1) src |= size_t{1} << order[q];
+        d[e] = o.m[src];
+    }
+    return true;
+}
+
+// Product of two diagonals given over ascending tile bits: the table over the union.
+static void mul_tables(std::vector<uint32_t>& bi, std::vector<cd>& di, const std::vector<uint32_t>& bj,
+                       const std::vector<cd>& dj) {
+    uint32_t uni = 0;
+    for (uint32_t b : bi) uni |= 1u << b;
+    for (uint32_t b : bj) uni |= 1u << b;
+    std::vector<uint32_t> ub;
+    for (uint32_t b = 0; b < 32; ++b)
+        if ((uni >> b) & 1) ub.push_back(b);
+    std::vector<cd> du(size_t{1} << ub.size());
+    for (size_t e = 0; e < du.size(); ++e) {
+        size_t ei = 0, ej = 0;
+        for (size_t q = 0; q < ub.size(); ++q) {
+            if (!((e >> q) & 1)) continue;
+            const auto pi = std::find(bi.begin(), bi.end(), ub[q]);
+            if (pi != bi.end()) ei |= size_t{1} << (pi - bi.begin());
+            const auto pj = std::find(bj.begin(), bj.end(), ub[q]);
+            if (pj != bj.end()) ej |= size_t{1} << (pj - bj.begin());
+        }
+        du[e] = di[ei] * dj[ej];
+    }
+    bi = std::move(ub);
+    di = std::move(du);
+}
+
+// Runs of diagonal work (phases such as the controlled phases of a QFT, diagonal blocks)
+// become one diagonal table over the union of their tile bits: an op joins an earlier
+// diagonal op when every op in between commutes with it (no dense target on its bits) and
+// the union stays within max_bits.  Ops with the same out-of-tile predicate merge into the
+// table itself.  With dyn_terms a phase gated by other out-of-tile qubits joins as a term
+// that the kernel multiplies into the table at the start of each tile where those qubits are
+// all 1 (a group whose own predicate differs turns into such terms when it is made of phases
+// only).  Each merge removes a pass over the tile's amplitudes for a table entry lookup.
+static void merge_diagonal_runs(std::vector<LocalOp>& ops, uint32_t max_bits, bool dyn_terms) {
+    std::vector<char> dead(ops.size(), 0);
+    std::vector<uint32_t> bi, bj;
+    std::vector<cd> di, dj;
+    uint32_t dyn_groups = 0, dyn_entries = 0;
+    auto mask_of = [](const std::vector<uint32_t>& bits) {
+        uint32_t mk = 0;
+        for (uint32_t b : bits) mk |= 1u << b;
+        return mk;
+    };
+    for (size_t i = 0; i < ops.size(); ++i) {
+        if (dead[i] || !diagonal_form(ops[i], bi, di)) continue;
+        uint64_t gc = ops[i].gcmask;
+        std::vector<DynTerm> dyn;
+        std::vector<DynTerm> phases;   // the group as phase terms while it is made of phases
+        bool only_phases = ops[i].kind == kTilePhase;
+        if (only_phases) phases.push_back({gc, ops[i].lmask, ops[i].m[0]});
+        uint32_t merged = 0;
+        uint32_t blocked = 0;   // tile bits a dense op between i and j targets
+        for (size_t j = i + 1; j < ops.size(); ++j) {
+            if (dead[j]) continue;
+            const LocalOp& q = ops[j];
+            if (diagonal_form(q, bj, dj)) {
+                const uint32_t mj = mask_of(bj);
+                const uint32_t uni = mask_of(bi) | mj;
+                const uint32_t width = static_cast<uint32_t>(__builtin_popcount(uni));
+                const bool fits = !(mj & blocked) && width <= max_bits &&
+                                  (dyn.empty() || dyn_entries + (1u << width) <= kRegMaxDynEntries);
+                if (fits && q.gcmask == gc) {
+                    mul_tables(bi, di, bj, dj);
+                    if (q.kind == kTilePhase) phases.push_back({q.gcmask, q.lmask, q.m[0]});
+                    else only_phases = false;
+                    dead[j] = 1;
+                    ++merged;
+                    continue;
+                }
+                // a gated phase as a per-tile term (table entries within the pass's budget)
+                const bool room = dyn_entries + (1u << width) <= kRegMaxDynEntries &&
+                                  (!dyn.empty() || dyn_groups < kRegMaxDyn) &&
+                                  dyn.size() + (gc ? phases.size() : 0) < kRegMaxDynTerms;
+                if (fits && dyn_terms && q.kind == kTilePhase && room && (gc == 0 || only_phases)) {
+                    if (gc != 0) {   // the group so far becomes terms over an identity table
+                        dyn = phases;
+                        std::fill(di.begin(), di.end(), cd{1, 0});
+                        gc = 0;
+                    }
+                    const std::vector<cd> ones(size_t{1} << bj.size(), cd{1, 0});
+                    mul_tables(bi, di, bj, ones);
+                    if (q.gcmask) dyn.push_back({q.gcmask, q.lmask, q.m[0]});
+                    else mul_tables(bi, di, bj, dj);
+                    phases.push_back({q.gcmask, q.lmask, q.m[0]});
+                    dead[j] = 1;
+                    ++merged;
+                    continue;
+                }
+            }
+            // q stays: later diagonal work may pass it only on bits it does not target
+            if (q.kind == kTileDense)
+                for (uint32_t b : q.lt) blocked |= 1u << b;
+        }
+        if (!merged) continue;   // a lone op keeps its own (cheaper) form
+        LocalOp& o = ops[i];
+        o.kind = kTileDiag;
+        o.lt = bi;
+        o.lmask = 0;
+        o.gcmask = gc;
+        o.m = di;
+        o.dyn = std::move(dyn);
+        if (!o.dyn.empty()) {
+            ++dyn_groups;
+            dyn_entries += 1u << o.lt.size();
+        }
+    }
+    size_t w = 0;
+    for (size_t i = 0; i < ops.size(); ++i) {
+        if (dead[i]) continue;
+        if (w != i) ops[w] = std::move(ops[i]);
+        ++w;
+    }
+    ops.resize(w);
+}
+
 // Peephole after inner fusion: a one-qubit dense or diagonal op (no controls) moves into the
 // next op touching its qubit — or, failing that, the previous one — when that op is a dense
 // block on it without controls (the ops in between do not touch the qubit, so they commute
@@ -263,7 +408,9 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
     std::vector<char> dead(ops.size(), 0);
     for (size_t i = 0; i < ops.size(); ++i) {
         LocalOp& p = ops[i];
-        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || p.variant) continue;
+        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || p.variant ||
+            !p.dyn.empty())
+            continue;
         const uint32_t a = p.lt[0];
         for (size_t j = i + 1; j < ops.size(); ++j) {
             if (dead[j]) continue;
@@ -316,7 +463,8 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
 
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
                                     const TileConfig& cfg, uint32_t max_select,
-                                    const std::vector<std::array<cd, 4>>* slot_mats) {
+                                    const std::vector<std::array<cd, 4>>* slot_mats,
+                                    uint32_t max_diag, bool dyn_terms) {
     LocalMap lm{cfg.L, item.hbits};
     std::vector<LocalOp> out;
     // a noise slot takes this state's matrix (identity when no table is given)
@@ -484,6 +632,7 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
         open.push_back(std::move(nb));
     }
     for (Open& b : open) emit_block(b);
+    merge_diagonal_runs(out, max_diag, dyn_terms);
     fold_single_qubit_ops(out, max_select);
     return out;
 }
@@ -690,6 +839,16 @@ namespace {
 void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vector<cd>& mats) {
     if (o.kind == kTilePhase || o.kind == kTileDiag) {
         mats.insert(mats.end(), o.m.begin(), o.m.end());
+        // per-tile terms: the factor, then {gcmask low 32 bits, gcmask high 32 bits * 64 +
+        // entry mask} as exact integers
+        for (const DynTerm& t : o.dyn) {
+            uint64_t em = 0;
+            for (size_t j = 0; j < o.lt.size(); ++j)
+                if ((t.lbits >> o.lt[j]) & 1) em |= uint64_t{1} << j;
+            mats.push_back(t.f);
+            mats.emplace_back(static_cast<double>(t.gcmask & 0xffffffffu),
+                              static_cast<double>((t.gcmask >> 32) * 64u + em));
+        }
         return;
     }
     const uint32_t k = static_cast<uint32_t>(o.lt.size());
@@ -740,7 +899,8 @@ RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m,
     if (o.kind == kTilePhase) {
         r.kind = kRegPhase;
     } else if (o.kind == kTileDiag) {
-        r.kind = kRegDiag;
+        r.kind = o.dyn.empty() ? kRegDiag : kRegDiagDyn;
+        r.nterm = static_cast<uint8_t>(o.dyn.size());
         for (uint32_t j = 0; j < k; ++j) {
             const uint32_t b = o.lt[j];
             r.loc[j] = static_cast<uint8_t>((S >> b) & 1 ? ridx[b] : (0x80 | tidx[b]));
@@ -756,7 +916,8 @@ RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m,
 
 bool same_shape(const LocalOp& a, const LocalOp& b) {
     return a.kind == b.kind && a.lt == b.lt && a.lmask == b.lmask && a.gcmask == b.gcmask &&
-           a.sel == b.sel && a.m.size() == b.m.size() && a.variant == b.variant;
+           a.sel == b.sel && a.m.size() == b.m.size() && a.variant == b.variant &&
+           a.dyn.size() == b.dyn.size();
 }
 
 bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates,
@@ -767,9 +928,10 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
     const std::vector<std::array<cd, 4>>* slots0 =
         state_slots && !state_slots->empty() ? &(*state_slots)[0] : nullptr;
-    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select, slots0);
+    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true);
     for (const LocalOp& o : ops)
-        if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : 4u)) return false;
+        if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : kRegMaxDiag))
+            return false;
     std::vector<Use> use;
     for (const LocalOp& o : ops) use.push_back(op_use(o));
 
@@ -829,6 +991,8 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     // records and the first state's matrices
     std::vector<RegOp> rec;
     std::vector<cd> mats;
+    std::vector<uint32_t> dyn_rec;
+    uint32_t dyn_entries = 0;
     for (const auto& [i, l] : seq) {
         if (i < 0) {
             RegOp r{};
@@ -838,16 +1002,24 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             rec.push_back(r);
             continue;
         }
-        rec.push_back(make_record(ops[i], lays[l], lay_sets[l], m, static_cast<uint32_t>(mats.size())));
+        RegOp r = make_record(ops[i], lays[l], lay_sets[l], m, static_cast<uint32_t>(mats.size()));
+        if (r.kind == kRegDiagDyn) {
+            r.dyn_off = static_cast<uint16_t>(dyn_entries);
+            dyn_entries += 1u << r.k;
+            dyn_rec.push_back(static_cast<uint32_t>(rec.size()));
+        }
+        rec.push_back(r);
         append_matrices(ops[i], lays[l], lay_sets[l], mats);
     }
-    if (rec.size() > kRegMaxRecords || lays.size() > kRegMaxLayouts || mats.size() > kRegMaxMatrix)
+    if (rec.size() > kRegMaxRecords || lays.size() > kRegMaxLayouts || mats.size() > kRegMaxMatrix ||
+        dyn_rec.size() > kRegMaxDyn || dyn_entries > kRegMaxDynEntries)
         return false;
     const size_t n_mat = mats.size();
     // every further state: same records, its own slot matrices
     if (state_slots) {
         for (size_t b = 1; b < state_slots->size(); ++b) {
-            const std::vector<LocalOp> ob = pass_local_ops(item, gates, cfg, max_select, &(*state_slots)[b]);
+            const std::vector<LocalOp> ob =
+                pass_local_ops(item, gates, cfg, max_select, &(*state_slots)[b], kRegMaxDiag, true);
             if (ob.size() != ops.size()) return false;
             for (size_t i = 0; i < ops.size(); ++i)
                 if (!same_shape(ops[i], ob[i])) return false;
@@ -867,6 +1039,9 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     pass.n_mat = static_cast<uint32_t>(n_mat);
     pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
     pass.sync_tiles = sync_tiles ? 1u : 0u;
+    pass.n_dyn = static_cast<uint32_t>(dyn_rec.size());
+    pass.dyn_entries = dyn_entries;
+    for (size_t d = 0; d < dyn_rec.size(); ++d) pass.dyn_rec[d] = static_cast<uint8_t>(dyn_rec[d]);
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());
     layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());
     mats_out.insert(mats_out.end(), mats.begin(), mats.end());

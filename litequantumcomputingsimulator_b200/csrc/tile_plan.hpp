@@ -27,6 +27,15 @@ struct PlanItem {
 std::vector<PlanItem> plan_tiles(const std::vector<GateDesc>& gates, uint32_t n,
                                  const TileConfig& cfg);
 
+// A phase factor f on the amplitudes whose tile-local bits lbits are all 1, applied only in
+// tiles whose out-of-tile qubits gcmask are all 1: one term of a diagonal whose table is
+// built per tile.
+struct DynTerm {
+    uint64_t gcmask = 0;
+    uint32_t lbits = 0;
+    cd f{1, 0};
+};
+
 // One operation of a pass in tile-local bits, before it is encoded for a kernel.
 struct LocalOp {
     uint8_t kind = kTileDense;      // kTileDense, kTileDiag or kTilePhase
@@ -37,15 +46,19 @@ struct LocalOp {
     bool variant = false;           // contains a noise slot: the matrices differ per state
     std::vector<cd> m;              // dense: 2^k x 2^k, diagonal: 2^k, phase: the factor;
                                     // with sel, one such block per selector value
+    std::vector<DynTerm> dyn;       // diagonal: gated phase terms multiplied into m per tile
 };
 
 // The operations of one pass in program order, neighbouring gates fused into blocks of at
 // most cfg.inner local qubits.  A block may take gates controlled by up to max_select
 // qubits outside the tile: those bits are constant over a tile, so the block becomes one
 // matrix per value of them, picked per tile.
+// Runs of commuting diagonal work merge into diagonals of at most max_diag tile bits; with
+// dyn_terms, phases gated by other out-of-tile qubits join them as per-tile terms.
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
                                     const TileConfig& cfg, uint32_t max_select,
-                                    const std::vector<std::array<cd, 4>>* slot_mats = nullptr);
+                                    const std::vector<std::array<cd, 4>>* slot_mats = nullptr,
+                                    uint32_t max_diag = kTileMaxK, bool dyn_terms = false);
 
 // Append the tile operations of one pass to ops_out (matrices to arena) and fill `pass`.
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,
