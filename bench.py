@@ -691,25 +691,26 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     except Exception as ex:  # noqa: BLE001
         out["costmodel_error"] = str(ex)
 
-    # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets in one launch
-    # batch): the first call builds the plan and captures its CUDA graph, the timed call
-    # replays it with new parameters; against direct launches, the plain one-set-at-a-time
-    # adjoint and the reference's parameter-shift method run on the GPU
+    # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets per call, the
+    # default resident count: as many sets as keep their states in L2, 32 here): the first
+    # call builds the plan and captures its CUDA graph, the timed call replays it with new
+    # parameters; against direct launches, the plain one-set-at-a-time adjoint and the
+    # reference's parameter-shift method run on the GPU
     try:
         pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
         ham = W.random_hamiltonian(16, 500, seed=12)
         sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
         sets2 = W.random_parameter_sets(pc.num_parameters(), 256, seed=14)
-        lq.algorithms.adjoint_gradient(ham, pc, sets, max_resident=256)
+        lq.algorithms.adjoint_gradient(ham, pc, sets)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        lq.algorithms.adjoint_gradient(ham, pc, sets2, max_resident=256)
+        lq.algorithms.adjoint_gradient(ham, pc, sets2)
         t_b = time.perf_counter() - t0
         os.environ["LQCS_GRAPHS"] = "0"
         try:
             lq.algorithms.adjoint_gradient(ham, pc, sets[:1], max_resident=1)
             t0 = time.perf_counter()
-            lq.algorithms.adjoint_gradient(ham, pc, sets2, max_resident=256)
+            lq.algorithms.adjoint_gradient(ham, pc, sets2)
             t_d = time.perf_counter() - t0
             t0 = time.perf_counter()
             for b in range(16):

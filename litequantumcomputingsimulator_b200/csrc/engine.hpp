@@ -196,6 +196,12 @@ struct Hamiltonian {
     std::vector<PauliMasks> terms;
 };
 Hamiltonian decode_hamiltonian(const lqcs_hamiltonian* h, uint32_t n);
+// A Hamiltonian on the device in the grouped form launch_apply_hamiltonian reads.
+struct HamiltonianDev {
+    DeviceBuffer terms, groups;
+    uint32_t n_terms = 0;
+    void upload(const Hamiltonian& h, uint32_t n);
+};
 double energy(lqcs_state& st, const Hamiltonian& h);
 // Decode a parametric circuit; parameterised gates must be RX, RY, RZ or rp without controls.
 void check_pc(const lqcs_parametric_circuit* pc, std::vector<GateDesc>& tmpl,

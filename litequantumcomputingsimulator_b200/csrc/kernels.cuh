@@ -140,9 +140,13 @@ struct PauliTermDev {
     uint64_t zy;
     double2 coeff;   // c_t * i^{n_y}
 };
+// Tile bits of the Hamiltonian apply.  Its terms come grouped by x >> ham_tile_bits(n) (the
+// groups in any order, terms of a group contiguous); d_groups = {G, G group keys, G + 1 term
+// offsets}.  HamiltonianDev builds both.
+uint32_t ham_tile_bits(uint32_t n);
 void launch_apply_hamiltonian(const LaunchCtx& ctx, const double2* in, double2* out,
                               uint32_t n, uint32_t batch, const PauliTermDev* d_terms,
-                              uint32_t n_terms);
+                              const uint32_t* d_groups);
 // Per-state Re<a|b> -> d_out[b] for a batch of states.  d_partials holds at least
 // batch * 64 doubles.
 void launch_batched_inner_re_p(const LaunchCtx& ctx, const double2* a, const double2* b,

@@ -519,41 +519,72 @@ void launch_move_to_zero(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t
 // ---------------------------------------------------------------- Hamiltonian apply
 // (H psi)[i] = sum_t c_t i^{n_y,t} (-1)^{popcount((i ^ x_t) & zy_t)} psi[i ^ x_t]
 // (the action of P on a basis state, src/backend/statevector.cpp:52-53).
+//
+// Tiled over the state: a CTA owns one output tile of 2^ml amplitudes (its index bits above
+// ml fixed), and the terms come sorted by the bits of x above ml in groups: groups[0] = G,
+// then G group keys g (x >> ml), then G + 1 term offsets.  For each group the CTA stages the
+// one source tile all its terms read (output tile ^ g) in shared memory and gathers from
+// there, so a source amplitude crosses L2 once per output tile and group instead of once per
+// term.
+uint32_t ham_tile_bits(uint32_t n) { return std::min<uint32_t>(n, 11); }
+
+template <int PER>
 __global__ void __launch_bounds__(256) k_apply_ham(const double2* __restrict__ in,
-                                                   double2* __restrict__ out, uint64_t len,
+                                                   double2* __restrict__ out, uint32_t n,
+                                                   uint32_t ml,
                                                    const PauliTermDev* __restrict__ terms,
-                                                   uint32_t n_terms) {
-    extern __shared__ PauliTermDev sterms[];
-    for (uint32_t t = threadIdx.x; t < n_terms; t += blockDim.x) sterms[t] = terms[t];
-    __syncthreads();
+                                                   const uint32_t* __restrict__ groups) {
+    extern __shared__ double2 src_tile[];
+    const uint64_t len = uint64_t{1} << n;
+    const uint32_t T = 1u << ml;
     const double2* src = in + static_cast<uint64_t>(blockIdx.y) * len;
     double2* dst = out + static_cast<uint64_t>(blockIdx.y) * len;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < len;
-         i += stride) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (uint32_t t = 0; t < n_terms; ++t) {
-            const PauliTermDev pt = sterms[t];
-            const uint64_t j = i ^ pt.x;
-            const double sg = parity_sign(j & pt.zy);
-            acc = cmad(cscale(pt.coeff, sg), __ldg(src + j), acc);
+    const uint64_t out_hi = blockIdx.x;
+    const uint32_t n_groups = __ldg(groups);
+    const uint32_t* keys = groups + 1;
+    const uint32_t* offs = keys + n_groups;
+    double2 acc[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) acc[j] = make_double2(0.0, 0.0);
+    for (uint32_t k = 0; k < n_groups; ++k) {
+        const uint64_t g = __ldg(keys + k);
+        const uint32_t t0 = __ldg(offs + k), t1 = __ldg(offs + k + 1);
+        __syncthreads();          // the previous group's gathers are done
+        const double2* row = src + ((out_hi ^ g) << ml);
+        for (uint32_t l = threadIdx.x; l < T; l += blockDim.x) src_tile[l] = __ldcg(row + l);
+        __syncthreads();
+        for (uint32_t t = t0; t < t1; ++t) {
+            const uint64_t x = __ldg(&terms[t].x), zy = __ldg(&terms[t].zy);
+            const double2 c = __ldg(&terms[t].coeff);
+            const uint32_t xl = static_cast<uint32_t>(x) & (T - 1u);
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                const uint32_t l = threadIdx.x + j * blockDim.x;
+                const uint64_t jj = ((out_hi << ml) | l) ^ x;
+                const double sg = (__popcll(jj & zy) & 1) ? -1.0 : 1.0;
+                acc[j] = cmad(make_double2(sg * c.x, sg * c.y), src_tile[l ^ xl], acc[j]);
+            }
         }
-        dst[i] = acc;
     }
+#pragma unroll
+    for (int j = 0; j < PER; ++j) dst[(out_hi << ml) | (threadIdx.x + j * blockDim.x)] = acc[j];
 }
 
 void launch_apply_hamiltonian(const LaunchCtx& ctx, const double2* in, double2* out,
                               uint32_t n, uint32_t batch, const PauliTermDev* d_terms,
-                              uint32_t n_terms) {
-    const uint64_t len = uint64_t{1} << n;
-    const uint32_t nb = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(
-        (len + 255) / 256, static_cast<uint64_t>(ctx.num_sms) * 8 / std::max(1u, batch) + 1)));
-    const size_t smem = sizeof(PauliTermDev) * n_terms;
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_apply_ham, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
+                              const uint32_t* d_groups) {
+    const uint32_t ml = ham_tile_bits(n);
+    const uint32_t T = 1u << ml;
+    const uint32_t threads = std::min<uint32_t>(256, T);
+    const uint32_t per = T / threads;
+    const dim3 grid(1u << (n - ml), batch);
+    const size_t smem = sizeof(double2) * T;
+    switch (per) {
+        case 1: k_apply_ham<1><<<grid, threads, smem, ctx.stream>>>(in, out, n, ml, d_terms, d_groups); break;
+        case 2: k_apply_ham<2><<<grid, threads, smem, ctx.stream>>>(in, out, n, ml, d_terms, d_groups); break;
+        case 4: k_apply_ham<4><<<grid, threads, smem, ctx.stream>>>(in, out, n, ml, d_terms, d_groups); break;
+        default: k_apply_ham<8><<<grid, threads, smem, ctx.stream>>>(in, out, n, ml, d_terms, d_groups); break;
     }
-    k_apply_ham<<<dim3(nb, batch), 256, smem, ctx.stream>>>(in, out, len, d_terms, n_terms);
     check_launch("apply_hamiltonian");
 }
 

@@ -279,6 +279,24 @@ def test_adjoint_matches_parameter_shift_and_fd(ref, n):
         assert abs(g[k] - (ep - em) / (2 * hstep)) < 1e-6
 
 
+@pytest.mark.parametrize("n", [12, 14])
+def test_adjoint_hamiltonian_over_tiles(ref, n):
+    """The Hamiltonian apply stages 2^11-amplitude source tiles grouped by the high bits of
+    each term's X mask: energies and gradients at 12 and 14 qubits (2 and 8 groups) match the
+    reference, batched (default resident count) as one set at a time."""
+    pc, _ = W.random_pauli_ansatz(n, 12, seed=n + 20, max_w=8)
+    h = W.random_hamiltonian(n, 60, seed=n + 21)
+    sets = W.random_parameter_sets(pc.num_parameters(), 5, seed=n + 22)
+    e_b, g_b = lq.algorithms.adjoint_gradient(h, pc, sets)
+    for b in (0, 4):
+        e_ref = ref.expectation(ref.run_statevector(pc.bind(sets[b])), h)
+        assert abs(e_b[b] - e_ref) < 1e-11
+        want = ref.parameter_shift_gradient(h, pc, sets[b])
+        assert np.max(np.abs(g_b[b] - want)) < 1e-9
+        e1, g1 = lq.algorithms.adjoint_gradient(h, pc, sets[b])
+        assert abs(e1 - e_b[b]) < 1e-12 and np.max(np.abs(g1 - g_b[b])) < 1e-12
+
+
 def test_adjoint_batched_equals_single(ref):
     pc, _ = W.random_pauli_ansatz(8, 24, seed=8)
     h = W.random_hamiltonian(8, 40, seed=9)
@@ -400,10 +418,10 @@ def test_release_caches_frees_plan_memory(ref):
     sets = W.random_parameter_sets(pc.num_parameters(), 64, seed=5)
     lq.algorithms.release_caches()
     free0 = torch.cuda.mem_get_info()[0]
-    e1, g1 = lq.algorithms.adjoint_gradient(h, pc, sets)
+    e1, g1 = lq.algorithms.adjoint_gradient(h, pc, sets, max_resident=64)
     held = free0 - torch.cuda.mem_get_info()[0]
     assert held >= 2 * 64 * (16 << 16)           # two resident batches of 64 states
     lq.algorithms.release_caches()
     assert torch.cuda.mem_get_info()[0] - free0 > -(16 << 20)
-    e2, g2 = lq.algorithms.adjoint_gradient(h, pc, sets)   # rebuilt after the release
+    e2, g2 = lq.algorithms.adjoint_gradient(h, pc, sets, max_resident=64)   # rebuilt
     assert np.array_equal(e1, e2) and np.array_equal(g1, g2)

@@ -78,6 +78,45 @@ def test_tile_brickwork_and_qft_vs_reference(ref, tile_env, inner, reg):
 
 
 @pytest.mark.parametrize("reg", [1, 0])
+@pytest.mark.parametrize("n", [13, 16])
+def test_diagonal_runs_and_gated_phases(port, tile_env, n, reg):
+    """Runs of phases and diagonals between a few dense gates: merged into tables of up to 6
+    tile bits, with phases controlled from outside the tile as per-tile terms (register
+    passes) — results must not depend on the merge."""
+    tile_env(12, 5, 2, reg)
+    rng = np.random.default_rng(n + 10 * reg)
+    qc = lq.QuantumCircuit(n)
+    for step in range(260):
+        a, b, c = (int(x) for x in rng.permutation(n)[:3])
+        k = int(rng.integers(9))
+        if step % 23 == 0 or k == 0:
+            qc.h(a)
+        elif k == 1:
+            qc.cp(float(rng.uniform(0, 6.3)), a, b)
+        elif k == 2:
+            qc.rzz(float(rng.uniform(0, 6.3)), a, b)
+        elif k == 3:
+            qc.mcp(float(rng.uniform(0, 6.3)), [a, b], c)
+        elif k == 4:
+            qc.cz(a, b)
+        elif k == 5:
+            qc.crz(float(rng.uniform(0, 6.3)), a, b)
+        elif k == 6:
+            qc.t(a)
+        elif k == 7:
+            qc.rz(float(rng.uniform(0, 6.3)), a)
+        else:
+            qc.u(*(float(x) for x in rng.uniform(0, 6.3, 3)), a)
+    init = W.gaussian_state(n, seed=n)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+    # the QFT's phase ladders: every pass holds long runs of gated phases
+    q = lq.algorithms.qft(n)
+    want = port.run_statevector(q, fuse=False, state=init)
+    assert np.max(np.abs(run(q, TILE, init) - want)) < TOL
+
+
+@pytest.mark.parametrize("reg", [1, 0])
 def test_tile_barrier_and_wide_gates(port, tile_env, reg):
     tile_env(12, 5, 2, reg)
     n = 14
