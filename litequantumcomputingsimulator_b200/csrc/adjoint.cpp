@@ -159,6 +159,87 @@ namespace {
 // terms and the per-set buffers, on a stream of its own.  A call only uploads the new
 // (cos, sin) tables, so the launch sequence of a batch of nb sets never changes: it is
 // captured once as a CUDA graph and replayed (LQCS_GRAPHS=0: launched directly).
+// One launch of the forward or backward sweep: a rotation tile pass (step < 0; its ops at
+// op_off in d_rot_ops) or one step launched on its own.
+struct Segment {
+    int step = -1;
+    RotTilePass pass{};
+    uint32_t op_off = 0;
+};
+
+// Greedy rotation tile passes over a run of parameterised steps, in the order given: a
+// rotation joins the open pass while the X bits above L of its rotations fit the m - L free
+// tile slots; a rotation whose own X bits do not fit runs on its own.
+void plan_rotation_passes(const std::vector<const GateStep*>& run,
+                          const std::vector<size_t>& index, uint32_t n, uint32_t m, uint32_t L,
+                          std::vector<Segment>& segs, std::vector<RotTileOp>& all_ops) {
+    const uint64_t low = (uint64_t{1} << L) - 1u;
+    const uint32_t slots = m - L;
+    uint64_t H = 0;
+    std::vector<const GateStep*> cur;
+    auto close = [&] {
+        if (cur.empty()) return;
+        for (uint32_t q = L; q < n && static_cast<uint32_t>(__builtin_popcountll(H)) < slots; ++q)
+            H |= uint64_t{1} << q;
+        Segment sg;
+        sg.pass.m = m;
+        sg.pass.L = L;
+        sg.pass.h = slots;
+        sg.pass.n_ops = static_cast<uint32_t>(cur.size());
+        uint32_t loc[64] = {};
+        for (uint32_t q = 0; q < L; ++q) loc[q] = q;
+        uint32_t i = 0;
+        for (uint32_t q = 0; q < n; ++q) {
+            if ((H >> q) & 1) {
+                sg.pass.hbits[i] = q;
+                loc[q] = L + i;
+                ++i;
+            }
+        }
+        const uint64_t tile = H | low;
+        auto local = [&](uint64_t mask) {
+            uint32_t r = 0;
+            for (uint32_t q = 0; q < n; ++q)
+                if (((mask & tile) >> q) & 1) r |= 1u << loc[q];
+            return r;
+        };
+        sg.op_off = static_cast<uint32_t>(all_ops.size());
+        for (const GateStep* st : cur) {
+            RotTileOp op{};
+            op.x_loc = local(st->gen.x);
+            op.zy_loc = local(st->gen.zy);
+            op.zy_out = st->gen.zy & ~tile;
+            op.param = static_cast<uint32_t>(st->param);
+            op.n_y = st->gen.n_y;
+            all_ops.push_back(op);
+        }
+        segs.push_back(sg);
+        cur.clear();
+        H = 0;
+    };
+    for (size_t r = 0; r < run.size(); ++r) {
+        const uint64_t need = run[r]->gen.x & ~low;
+        if (static_cast<uint32_t>(__builtin_popcountll(need)) > slots) {
+            close();
+            Segment own;
+            own.step = static_cast<int>(index[r]);
+            segs.push_back(own);
+            continue;
+        }
+        if (!cur.empty() && (static_cast<uint32_t>(__builtin_popcountll(H | need)) > slots ||
+                             cur.size() == kRotMaxOps))
+            close();
+        H |= need;
+        cur.push_back(run[r]);
+    }
+    close();
+}
+
+int env_or(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+
 struct AdjointPlan {
     uint64_t key = 0;
     uint32_t n = 0, R = 0;
@@ -167,6 +248,9 @@ struct AdjointPlan {
     HamiltonianDev ham;
     std::unique_ptr<lqcs_state> psi, lam;
     DeviceBuffer d_cs, d_csi, d_part, d_energy, d_grad;
+    // rotation tile passes (empty: one launch per step)
+    std::vector<Segment> fwd_segs, bwd_segs;
+    DeviceBuffer d_rot_ops, d_rot_part;
     cudaStream_t stream = nullptr;
     std::map<uint32_t, std::pair<cudaGraphExec_t, uint64_t>> graphs;   // nb -> (graph, kernels)
 
@@ -180,17 +264,44 @@ struct AdjointPlan {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    void forward_step(const GateStep& s, uint32_t nb) const {
+        const LaunchCtx& ctx = psi->ctx;
+        if (s.param >= 0) {
+            launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y,
+                                          d_cs.as<double2>() + static_cast<uint64_t>(s.param) * R);
+        } else {
+            s.fwd.launch(ctx, psi->d(), n, nb);
+        }
+    }
+
+    void backward_step(const GateStep& s, uint32_t nb) const {
+        const LaunchCtx& ctx = psi->ctx;
+        if (s.param >= 0) {
+            launch_batched_pauli_im_p(ctx, lam->d(), psi->d(), n, nb, s.gen.x, s.gen.zy,
+                                      s.gen.n_y, d_part.as<double>(),
+                                      d_grad.as<double>() + s.param, np);
+            const double2* inv = d_csi.as<double2>() + static_cast<uint64_t>(s.param) * R;
+            launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+            launch_pauli_rotation_batched(ctx, lam->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
+        } else {
+            s.inv.launch(ctx, psi->d(), n, nb);
+            s.inv.launch(ctx, lam->d(), n, nb);
+        }
+    }
+
     // The launch sequence of one batch of nb sets on this plan's stream.
     void enqueue(uint32_t nb) const {
         const LaunchCtx& ctx = psi->ctx;
         const uint64_t len = uint64_t{1} << n;
+        const RotTileOp* rot_ops = d_rot_ops.as<RotTileOp>();
         launch_set_basis(ctx, psi->d(), n, nb, 0);
-        for (const GateStep& s : steps) {
-            if (s.param >= 0) {
-                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y,
-                                              d_cs.as<double2>() + static_cast<uint64_t>(s.param) * R);
-            } else {
-                s.fwd.launch(ctx, psi->d(), n, nb);
+        if (fwd_segs.empty()) {
+            for (const GateStep& s : steps) forward_step(s, nb);
+        } else {
+            for (const Segment& sg : fwd_segs) {
+                if (sg.step >= 0) forward_step(steps[sg.step], nb);
+                else launch_rot_tile_fwd(ctx, psi->d(), n, nb, sg.pass, rot_ops + sg.op_off,
+                                         d_cs.as<double2>(), R);
             }
         }
         if (ham.n_terms == 0) {
@@ -201,20 +312,68 @@ struct AdjointPlan {
         }
         launch_batched_inner_re_p(ctx, psi->d(), lam->d(), n, nb, d_part.as<double>(),
                                   d_energy.as<double>());
-        for (size_t i = steps.size(); i-- > 0;) {
-            const GateStep& s = steps[i];
-            if (s.param >= 0) {
-                launch_batched_pauli_im_p(ctx, lam->d(), psi->d(), n, nb, s.gen.x, s.gen.zy,
-                                          s.gen.n_y, d_part.as<double>(),
-                                          d_grad.as<double>() + s.param, np);
-                const double2* inv = d_csi.as<double2>() + static_cast<uint64_t>(s.param) * R;
-                launch_pauli_rotation_batched(ctx, psi->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
-                launch_pauli_rotation_batched(ctx, lam->d(), n, nb, s.gen.x, s.gen.zy, s.gen.n_y, inv);
-            } else {
-                s.inv.launch(ctx, psi->d(), n, nb);
-                s.inv.launch(ctx, lam->d(), n, nb);
+        if (bwd_segs.empty()) {
+            for (size_t i = steps.size(); i-- > 0;) backward_step(steps[i], nb);
+        } else {
+            for (const Segment& sg : bwd_segs) {
+                if (sg.step >= 0) backward_step(steps[sg.step], nb);
+                else launch_rot_tile_bwd(ctx, psi->d(), lam->d(), n, nb, sg.pass, rot_ops + sg.op_off,
+                                         d_cs.as<double2>(), R, d_rot_part.as<double>(),
+                                         d_grad.as<double>(), np);
             }
         }
+    }
+
+    // Rotation tile passes for both sweeps: forward tiles of 2^min(n, 12) amplitudes (one
+    // state in shared memory), backward 2^min(n, 11) (psi and lambda); qubits 0..2 stay in
+    // every tile so tile rows are 128-byte lines.  LQCS_ADJ_TILES=0 keeps one launch per step.
+    void plan_tiles() {
+        if (env_or("LQCS_ADJ_TILES", 1) == 0) return;
+        const uint32_t mf = std::min<uint32_t>(n, static_cast<uint32_t>(env_or("LQCS_ADJ_TILE_F", 12)));
+        const uint32_t mb = std::min<uint32_t>(n, static_cast<uint32_t>(env_or("LQCS_ADJ_TILE_B", 11)));
+        if (mf < 5 || mb < 5 || mf > kRotMaxBits || mb > kRotMaxBits) return;
+        const uint32_t L = 3;
+        std::vector<RotTileOp> ops;
+        std::vector<const GateStep*> run;
+        std::vector<size_t> idx;
+        auto flush = [&](std::vector<Segment>& segs, uint32_t m) {
+            plan_rotation_passes(run, idx, n, m, L, segs, ops);
+            run.clear();
+            idx.clear();
+        };
+        for (size_t i = 0; i < steps.size(); ++i) {
+            if (steps[i].param >= 0) {
+                run.push_back(&steps[i]);
+                idx.push_back(i);
+                continue;
+            }
+            flush(fwd_segs, mf);
+            Segment own;
+            own.step = static_cast<int>(i);
+            fwd_segs.push_back(own);
+        }
+        flush(fwd_segs, mf);
+        for (size_t i = steps.size(); i-- > 0;) {
+            if (steps[i].param >= 0) {
+                run.push_back(&steps[i]);
+                idx.push_back(i);
+                continue;
+            }
+            flush(bwd_segs, mb);
+            Segment own;
+            own.step = static_cast<int>(i);
+            bwd_segs.push_back(own);
+        }
+        flush(bwd_segs, mb);
+        uint32_t max_ops = 1;
+        for (const Segment& sg : bwd_segs)
+            if (sg.step < 0) max_ops = std::max(max_ops, sg.pass.n_ops);
+        d_rot_ops.ensure(sizeof(RotTileOp) * std::max<size_t>(1, ops.size()));
+        if (!ops.empty())
+            cuda_check(cudaMemcpy(d_rot_ops.ptr, ops.data(), sizeof(RotTileOp) * ops.size(),
+                                  cudaMemcpyHostToDevice),
+                       "H2D rotation passes");
+        d_rot_part.ensure(sizeof(double) * max_ops * R * (uint64_t{1} << (n - mb)));
     }
 
     void run(uint32_t nb) {
@@ -343,6 +502,7 @@ std::unique_ptr<AdjointPlan> build_plan(const std::vector<GateDesc>& tmpl,
     plan->psi = new_state(n, R, plan->stream);
     plan->lam = new_state(n, R, plan->stream);
     plan->ham.upload(h, n);
+    plan->plan_tiles();
     plan->d_cs.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
     plan->d_csi.ensure(sizeof(double2) * std::max<uint64_t>(1, np) * R);
     plan->d_part.ensure(sizeof(double) * 64 * R);

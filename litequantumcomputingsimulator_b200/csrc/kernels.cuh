@@ -147,6 +147,40 @@ uint32_t ham_tile_bits(uint32_t n);
 void launch_apply_hamiltonian(const LaunchCtx& ctx, const double2* in, double2* out,
                               uint32_t n, uint32_t batch, const PauliTermDev* d_terms,
                               const uint32_t* d_groups);
+// ---------------------------------------------------------------- rotation tile passes
+// A run of Pauli rotations applied to tiles of 2^m amplitudes in shared memory: local bit
+// j < L is qubit j, local bit L + i is qubit hbits[i] (ascending).  Every rotation's X mask
+// lies in the tile; its Z / Y bits outside the tile give a sign that is uniform per tile.
+constexpr uint32_t kRotThreads = 256;
+constexpr uint32_t kRotMaxBits = 12;
+constexpr uint32_t kRotMaxHigh = 16;
+constexpr uint32_t kRotMaxOps = 64;   // rotations per pass (staged in shared memory)
+constexpr uint32_t kRotMaxRows = (1u << kRotMaxBits) / kRotThreads;
+struct RotTileOp {
+    uint64_t zy_out;   // Z / Y bits outside the tile
+    uint32_t x_loc;    // X / Y bits, tile-local (0: diagonal rotation)
+    uint32_t zy_loc;   // Z / Y bits, tile-local
+    uint32_t param;    // row of the (cos, sin) of theta/2 table ([param][state])
+    uint32_t n_y;
+    uint32_t pad[2];
+};
+struct RotTilePass {
+    uint32_t m, L, h, n_ops;
+    uint32_t hbits[kRotMaxHigh];
+};
+size_t rot_tile_smem(uint32_t m, bool backward);
+void launch_rot_tile_fwd(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t nb,
+                         const RotTilePass& p, const RotTileOp* d_ops, const double2* d_cs,
+                         uint32_t R);
+// Backward pass: per rotation (in the order given) d_grad[state * np + param] =
+// Im<lambda|P|psi> before the rotation is undone on psi and lambda.  d_partials holds
+// n_ops * nb * 2^(n - m) doubles.
+void launch_rot_tile_bwd(const LaunchCtx& ctx, double2* psi, double2* lam, uint32_t n,
+                         uint32_t nb, const RotTilePass& p, const RotTileOp* d_ops,
+                         const double2* d_cs, uint32_t R, double* d_partials, double* d_grad,
+                         uint64_t np);
+void cuda_check_launch_attr(cudaError_t e);
+
 // Per-state Re<a|b> -> d_out[b] for a batch of states.  d_partials holds at least
 // batch * 64 doubles.
 void launch_batched_inner_re_p(const LaunchCtx& ctx, const double2* a, const double2* b,

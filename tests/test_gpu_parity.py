@@ -297,6 +297,34 @@ def test_adjoint_hamiltonian_over_tiles(ref, n):
         assert abs(e1 - e_b[b]) < 1e-12 and np.max(np.abs(g1 - g_b[b])) < 1e-12
 
 
+@pytest.mark.parametrize("n", [7, 13, 16])
+def test_adjoint_rotation_tile_passes(ref, monkeypatch, n):
+    """Runs of parameterised rotations go through shared-memory tile passes (forward and
+    backward, gradients summed over tiles); fixed gates and rotations whose X bits do not fit
+    a tile split the runs.  Energies and gradients agree with one launch per step and with
+    the reference's parameter-shift gradient."""
+    pc, _ = W.random_pauli_ansatz(n, 14, seed=n + 40, max_w=min(8, n))
+    pc.h(0)
+    pc.cx(1, n - 1)
+    pc.rp("X" * n, list(range(n)))   # X bits on every qubit: wider than any tile when n > 12
+    pc.ry(n - 1)
+    pc.s(2)
+    more, _ = W.random_pauli_ansatz(n, 9, seed=n + 41, max_w=min(8, n))
+    for inst in more.template().instructions():
+        pc.rp(inst.gate.pauli, list(inst.qubits))
+    h = W.random_hamiltonian(n, 30, seed=n + 42)
+    sets = W.random_parameter_sets(pc.num_parameters(), 6, seed=n + 43)
+    e_t, g_t = lq.algorithms.adjoint_gradient(h, pc, sets)
+    lq.algorithms.release_caches()
+    monkeypatch.setenv("LQCS_ADJ_TILES", "0")
+    e_s, g_s = lq.algorithms.adjoint_gradient(h, pc, sets)
+    lq.algorithms.release_caches()
+    assert np.max(np.abs(e_t - e_s)) < 1e-12
+    assert np.max(np.abs(g_t - g_s)) < 1e-12
+    want = ref.parameter_shift_gradient(h, pc, sets[2])
+    assert np.max(np.abs(g_t[2] - want)) < 1e-9
+
+
 def test_adjoint_batched_equals_single(ref):
     pc, _ = W.random_pauli_ansatz(8, 24, seed=8)
     h = W.random_hamiltonian(8, 40, seed=9)
