@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--fusion-width", type=int, default=0)
     ap.add_argument("--fusion-mode", type=int, default=0)
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
+    ap.add_argument("--extras", default=None,
+                    help="comma-separated extra legs to run (sweep, unfused, qft, trajectories, "
+                         "width6, autotune, ragged, dm, costmodel, adjoint); default all")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -472,264 +475,280 @@ def run_e2e(lq, qc, gate_bytes, args, dist=None, device=None, world=1):
 def run_extras(lq, W, N, n, sv, hbm_peak, args):
     import torch
     out = {}
+    legs = None if args.extras in (None, "all") else set(args.extras.split(","))
+
+    def want(name):
+        return legs is None or name in legs
+
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # per-target sweep: one U3 on target t, timed over R launches
-    sweep = {}
-    reps = 5
-    for t in range(n):
-        c = lq.QuantumCircuit(n)
-        c.u(0.3, 0.5, 0.7, t)
-        p = lq.simulator.CompiledCircuit(c, fuse_gates=False)
-        p.apply(sv)
+    if want("sweep"):
+        sweep = {}
+        reps = 5
+        for t in range(n):
+            c = lq.QuantumCircuit(n)
+            c.u(0.3, 0.5, 0.7, t)
+            p = lq.simulator.CompiledCircuit(c, fuse_gates=False)
+            p.apply(sv)
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            for _ in range(reps):
+                p.apply(sv)
+            e.record()
+            torch.cuda.synchronize()
+            ms = s.elapsed_time(e) / reps
+            sweep[t] = 32.0 * (1 << n) / (ms / 1e3) / 1e9
+        vals = list(sweep.values())
+        out["per_target_u3_gbs"] = {str(k): round(v, 1) for k, v in sweep.items()}
+        out["per_target_u3_min_frac"] = min(vals) / hbm_peak
+        out["per_target_u3_median_frac"] = statistics.median(vals) / hbm_peak
+
+    # unfused gate-by-gate path on the same brickwork (for the fusion speed-up)
+    if want("unfused"):
+        qc = W.brickwork(n, args.depth, args.seed)
+        plain = lq.simulator.CompiledCircuit(qc, fuse_gates=False)
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        for _ in range(reps):
-            p.apply(sv)
+        plain.apply(sv)
         e.record()
         torch.cuda.synchronize()
-        ms = s.elapsed_time(e) / reps
-        sweep[t] = 32.0 * (1 << n) / (ms / 1e3) / 1e9
-    vals = list(sweep.values())
-    out["per_target_u3_gbs"] = {str(k): round(v, 1) for k, v in sweep.items()}
-    out["per_target_u3_min_frac"] = min(vals) / hbm_peak
-    out["per_target_u3_median_frac"] = statistics.median(vals) / hbm_peak
-
-    # unfused gate-by-gate path on the same brickwork (for the fusion speed-up)
-    qc = W.brickwork(n, args.depth, args.seed)
-    plain = lq.simulator.CompiledCircuit(qc, fuse_gates=False)
-    torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    plain.apply(sv)
-    e.record()
-    torch.cuda.synchronize()
-    ms_plain = s.elapsed_time(e)
-    out["brickwork_unfused_gbs"] = W.alg_bytes(qc) / (ms_plain / 1e3) / 1e9
-    out["brickwork_unfused_ms"] = ms_plain
+        ms_plain = s.elapsed_time(e)
+        out["brickwork_unfused_gbs"] = W.alg_bytes(qc) / (ms_plain / 1e3) / 1e9
+        out["brickwork_unfused_ms"] = ms_plain
 
     # QFT(n) on a random state: the state is filled on the device side by a random circuit
     # would change the workload; instead the Gaussian state is uploaded once (not timed)
-    try:
-        qft = lq.algorithms.qft(n)
-        pq = lq.simulator.CompiledCircuit(qft, fuse_gates=True)
-        pq.apply(sv)
-        torch.cuda.synchronize()
-        s.record()
-        pq.apply(sv)
-        e.record()
-        torch.cuda.synchronize()
-        ms_q = s.elapsed_time(e)
-        out["qft_ms"] = ms_q
-        out["qft_gates"] = qft.num_instructions()
-        out["qft_gbs"] = W.alg_bytes(qft) / (ms_q / 1e3) / 1e9
-        out["qft_device_ops"] = pq.n_ops
-    except Exception as ex:  # noqa: BLE001
-        out["qft_error"] = str(ex)
+    if want("qft"):
+        try:
+            qft = lq.algorithms.qft(n)
+            pq = lq.simulator.CompiledCircuit(qft, fuse_gates=True)
+            pq.apply(sv)
+            torch.cuda.synchronize()
+            s.record()
+            pq.apply(sv)
+            e.record()
+            torch.cuda.synchronize()
+            ms_q = s.elapsed_time(e)
+            out["qft_ms"] = ms_q
+            out["qft_gates"] = qft.num_instructions()
+            out["qft_gbs"] = W.alg_bytes(qft) / (ms_q / 1e3) / 1e9
+            out["qft_device_ops"] = pq.n_ops
+        except Exception as ex:  # noqa: BLE001
+            out["qft_error"] = str(ex)
 
     # noisy trajectories: 26-qubit brickwork depth 20, depolarizing 1e-3 after each U3,
     # 1e-2 on both qubits after each CX, amplitude damping 1e-3 per qubit per layer; up to 64
     # resident per batch.  Fused driver: 128 trajectories (2 batches, a bounded sample of the
     # 1024-trajectory run); gate-by-gate driver: 16 trajectories, for the comparison.
-    try:
-        tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
-        warm = W.brickwork(12, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3))
-        sim = lq.StatevectorSimulator(seed=404, max_resident=64)
-        sim.run_registers(warm, 8)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        fused_regs = sim.run_registers(tq, 128)
-        dt = time.perf_counter() - t0
-        out["trajectories_26q_per_s"] = 128 / dt
-        out["trajectories_26q_sample"] = ("128 trajectories, 64 resident per batch (1 GiB each), "
-                                          "fused driver, host-timed")
-        os.environ["LQCS_TRAJ_FUSED"] = "0"
+    if want("trajectories"):
         try:
-            plain = lq.StatevectorSimulator(seed=404, max_resident=16)
-            plain.run_registers(warm, 8)
+            tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+            warm = W.brickwork(12, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3))
+            sim = lq.StatevectorSimulator(seed=404, max_resident=64)
+            sim.run_registers(warm, 8)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            plain_regs = plain.run_registers(tq, 16)
-            dtp = time.perf_counter() - t0
-        finally:
-            os.environ.pop("LQCS_TRAJ_FUSED", None)
-        out["trajectories_26q_plain_per_s"] = 16 / dtp
-        out["trajectories_26q_fused_speedup"] = (128 / dt) / (16 / dtp)
-        out["trajectories_26q_same_registers"] = bool((fused_regs[:16] == plain_regs).all())
-    except Exception as ex:  # noqa: BLE001
-        out["trajectories_error"] = str(ex)
+            fused_regs = sim.run_registers(tq, 128)
+            dt = time.perf_counter() - t0
+            out["trajectories_26q_per_s"] = 128 / dt
+            out["trajectories_26q_sample"] = ("128 trajectories, 64 resident per batch (1 GiB each), "
+                                              "fused driver, host-timed")
+            os.environ["LQCS_TRAJ_FUSED"] = "0"
+            try:
+                plain = lq.StatevectorSimulator(seed=404, max_resident=16)
+                plain.run_registers(warm, 8)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                plain_regs = plain.run_registers(tq, 16)
+                dtp = time.perf_counter() - t0
+            finally:
+                os.environ.pop("LQCS_TRAJ_FUSED", None)
+            out["trajectories_26q_plain_per_s"] = 16 / dtp
+            out["trajectories_26q_fused_speedup"] = (128 / dt) / (16 / dtp)
+            out["trajectories_26q_same_registers"] = bool((fused_regs[:16] == plain_regs).all())
+        except Exception as ex:  # noqa: BLE001
+            out["trajectories_error"] = str(ex)
 
     # wide fused blocks: 28-qubit brickwork depth 20 fused greedily to 6-qubit blocks, on the
     # FP64 tensor path (mma.sync.m8n8k4.f64) and on the FFMA kernel
-    try:
-        wq = W.brickwork(28, 20, seed=55)
-        wsv = lq.Statevector(28)
-        wprog = lq.simulator.CompiledCircuit(wq, True, 6, 1)
-        res = {}
-        for name, flag in (("dmma", "1"), ("ffma", "0")):
-            os.environ["LQCS_DENSE_MMA"] = flag
-            try:
-                wprog.apply(wsv)
-                torch.cuda.synchronize()
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record()
-                wprog.apply(wsv)
-                e.record()
-                torch.cuda.synchronize()
-                res[name] = s.elapsed_time(e)
-            finally:
-                os.environ.pop("LQCS_DENSE_MMA", None)
-        prof = wprog.profile(wsv)
-        k6 = [r for r in prof if r["kernel"] == "k_dense<6>"]
-        out["width6_28q_ms"] = {k: round(v, 2) for k, v in res.items()}
-        out["width6_28q_dmma_speedup"] = res["ffma"] / res["dmma"]
-        if k6:
-            out["width6_dmma_k6_tflops"] = (sum(r["alg_flops"] for r in k6) /
-                                            (sum(r["ms"] for r in k6) / 1e3) / 1e12)
-        del wsv
-    except Exception as ex:  # noqa: BLE001
-        out["width6_error"] = str(ex)
+    if want("width6"):
+        try:
+            wq = W.brickwork(28, 20, seed=55)
+            wsv = lq.Statevector(28)
+            wprog = lq.simulator.CompiledCircuit(wq, True, 6, 1)
+            res = {}
+            for name, flag in (("dmma", "1"), ("ffma", "0")):
+                os.environ["LQCS_DENSE_MMA"] = flag
+                try:
+                    wprog.apply(wsv)
+                    torch.cuda.synchronize()
+                    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s.record()
+                    wprog.apply(wsv)
+                    e.record()
+                    torch.cuda.synchronize()
+                    res[name] = s.elapsed_time(e)
+                finally:
+                    os.environ.pop("LQCS_DENSE_MMA", None)
+            prof = wprog.profile(wsv)
+            k6 = [r for r in prof if r["kernel"] == "k_dense<6>"]
+            out["width6_28q_ms"] = {k: round(v, 2) for k, v in res.items()}
+            out["width6_28q_dmma_speedup"] = res["ffma"] / res["dmma"]
+            if k6:
+                out["width6_dmma_k6_tflops"] = (sum(r["alg_flops"] for r in k6) /
+                                                (sum(r["ms"] for r in k6) / 1e3) / 1e12)
+            del wsv
+        except Exception as ex:  # noqa: BLE001
+            out["width6_error"] = str(ex)
 
     # autotuner: every candidate plan of a 28-qubit brickwork (depth 40) timed on the device;
     # the chosen plan against the default one
-    try:
-        aq = W.brickwork(28, 40, seed=66)
-        t0 = time.perf_counter()
-        tune = lq.simulator.autotune(aq)
-        out["autotune_28q_s"] = time.perf_counter() - t0
-        out["autotune_28q"] = [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()}
-                               for r in tune]
-        chosen = [r for r in tune if r["chosen"]]
-        default = [r for r in tune if r["planner"] == "register tile passes" and
-                   r["tile_bits"] == 12 and r["inner"] == 2]
-        if chosen and default:
-            out["autotune_28q_gain_vs_default"] = default[0]["ms"] / chosen[0]["ms"]
-    except Exception as ex:  # noqa: BLE001
-        out["autotune_error"] = str(ex)
+    if want("autotune"):
+        try:
+            aq = W.brickwork(28, 40, seed=66)
+            t0 = time.perf_counter()
+            tune = lq.simulator.autotune(aq)
+            out["autotune_28q_s"] = time.perf_counter() - t0
+            out["autotune_28q"] = [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()}
+                                   for r in tune]
+            chosen = [r for r in tune if r["chosen"]]
+            default = [r for r in tune if r["planner"] == "register tile passes" and
+                       r["tile_bits"] == 12 and r["inner"] == 2]
+            if chosen and default:
+                out["autotune_28q_gain_vs_default"] = default[0]["ms"] / chosen[0]["ms"]
+        except Exception as ex:  # noqa: BLE001
+            out["autotune_error"] = str(ex)
 
     # uneven qubit counts: 8 problems of 10..17 qubits (100 rp gates, 100 terms, 32 parameter
     # sets each) as one captured graph with concurrent branches, against the same problems
     # one call after another
-    try:
-        probs = []
-        for i, nq in enumerate(range(10, 18)):
-            pc_i, _ = W.random_pauli_ansatz(nq, 100, seed=200 + i)
-            probs.append((W.random_hamiltonian(nq, 100, seed=300 + i), pc_i))
-        def sets_for(seed):
-            return [W.random_parameter_sets(pc_i.num_parameters(), 32, seed=seed + j)
-                    for j, (h_i, pc_i) in enumerate(probs)]
-        lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, sets_for(1))])
-        for (h, pc_i), s in zip(probs, sets_for(1)):
-            lq.algorithms.adjoint_gradient(h, pc_i, s)
-        torch.cuda.synchronize()
-        s2 = sets_for(2)
-        t0 = time.perf_counter()
-        lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, s2)])
-        t_m = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        for (h, pc_i), s in zip(probs, s2):
-            lq.algorithms.adjoint_gradient(h, pc_i, s)
-        t_s = time.perf_counter() - t0
-        out["ragged_8x32_sets_per_s"] = 8 * 32 / t_m
-        out["ragged_sequential_sets_per_s"] = 8 * 32 / t_s
-        out["ragged_speedup"] = t_s / t_m
-    except Exception as ex:  # noqa: BLE001
-        out["ragged_error"] = str(ex)
+    if want("ragged"):
+        try:
+            probs = []
+            for i, nq in enumerate(range(10, 18)):
+                pc_i, _ = W.random_pauli_ansatz(nq, 100, seed=200 + i)
+                probs.append((W.random_hamiltonian(nq, 100, seed=300 + i), pc_i))
+            def sets_for(seed):
+                return [W.random_parameter_sets(pc_i.num_parameters(), 32, seed=seed + j)
+                        for j, (h_i, pc_i) in enumerate(probs)]
+            lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, sets_for(1))])
+            for (h, pc_i), s in zip(probs, sets_for(1)):
+                lq.algorithms.adjoint_gradient(h, pc_i, s)
+            torch.cuda.synchronize()
+            s2 = sets_for(2)
+            t0 = time.perf_counter()
+            lq.algorithms.adjoint_gradient_multi([(h, pc_i, s) for (h, pc_i), s in zip(probs, s2)])
+            t_m = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            for (h, pc_i), s in zip(probs, s2):
+                lq.algorithms.adjoint_gradient(h, pc_i, s)
+            t_s = time.perf_counter() - t0
+            out["ragged_8x32_sets_per_s"] = 8 * 32 / t_m
+            out["ragged_sequential_sets_per_s"] = 8 * 32 / t_s
+            out["ragged_speedup"] = t_s / t_m
+        except Exception as ex:  # noqa: BLE001
+            out["ragged_error"] = str(ex)
 
     # density-matrix backend: config-3 noise on a 13-qubit brickwork, depth 20 (rho as a
     # 26-qubit device state, 1 GiB), and the 10-qubit cross-check size
-    try:
-        for nq in (10, 13):
-            dq = W.brickwork(nq, 20, seed=88, noise=(1e-3, 1e-2, 1e-3))
-            dsim = lq.DensityMatrixSimulator()
-            dsim.run_density_matrix(W.brickwork(nq, 1, seed=1))
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            p = dsim.run_density_matrix(dq).probabilities()
-            out[f"dm_{nq}q_d20_s"] = time.perf_counter() - t0
-            out[f"dm_{nq}q_trace"] = float(p.sum())
-    except Exception as ex:  # noqa: BLE001
-        out["dm_error"] = str(ex)
+    if want("dm"):
+        try:
+            for nq in (10, 13):
+                dq = W.brickwork(nq, 20, seed=88, noise=(1e-3, 1e-2, 1e-3))
+                dsim = lq.DensityMatrixSimulator()
+                dsim.run_density_matrix(W.brickwork(nq, 1, seed=1))
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                p = dsim.run_density_matrix(dq).probabilities()
+                out[f"dm_{nq}q_d20_s"] = time.perf_counter() - t0
+                out[f"dm_{nq}q_trace"] = float(p.sum())
+        except Exception as ex:  # noqa: BLE001
+            out["dm_error"] = str(ex)
 
     # learned fusion cost model: trained on the engine's own per-operation timings of
     # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the
     # greedy plan of a held-out 32-qubit circuit (64 GiB state) are timed on the device
-    try:
-        from litequantumcomputingsimulator_b200 import costmodel as CM
-        train_set = [W.random_mix_circuit(nq, d, s) for nq, d, s in
-                     [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14)]]
-        t0 = time.perf_counter()
-        x, y = CM.collect(train_set)
-        t1 = time.perf_counter()
-        loss = CM.train(x, y, epochs=3000, lr=3e-3, seed=0)
-        t_train = time.perf_counter() - t1
-        out["costmodel_train_rows_x_epochs_per_s"] = y.size * 3000 / t_train
-        xi = np.repeat(x, max(1, 1_000_000 // max(1, len(x))), axis=0)
-        CM.predict(xi[:1024])
-        t1 = time.perf_counter()
-        CM.predict(xi)
-        out["costmodel_infer_rows_per_s"] = len(xi) / (time.perf_counter() - t1)
-        out["costmodel_train_rows"] = int(y.size)
-        out["costmodel_train_mse"] = loss
-        out["costmodel_collect_train_s"] = time.perf_counter() - t0
-        held = W.random_mix_circuit(32, 16, seed=777)
-        big = lq.Statevector(32)
-        res = {}
-        for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED)):
-            prog = lq.simulator.CompiledCircuit(held, True, 0, mode)
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            prog.apply(big)
-            e.record()
-            torch.cuda.synchronize()
-            res[name] = (s.elapsed_time(e), prog.n_ops)
-        out["costmodel_32q_greedy_ms"] = res["greedy"][0]
-        out["costmodel_32q_learned_ms"] = res["learned"][0]
-        out["costmodel_32q_ops"] = {"greedy": res["greedy"][1], "learned": res["learned"][1]}
-        out["costmodel_32q_speedup"] = res["greedy"][0] / res["learned"][0]
-        del big
-        torch.cuda.empty_cache()
-    except Exception as ex:  # noqa: BLE001
-        out["costmodel_error"] = str(ex)
+    if want("costmodel"):
+        try:
+            from litequantumcomputingsimulator_b200 import costmodel as CM
+            train_set = [W.random_mix_circuit(nq, d, s) for nq, d, s in
+                         [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14)]]
+            t0 = time.perf_counter()
+            x, y = CM.collect(train_set)
+            t1 = time.perf_counter()
+            loss = CM.train(x, y, epochs=3000, lr=3e-3, seed=0)
+            t_train = time.perf_counter() - t1
+            out["costmodel_train_rows_x_epochs_per_s"] = y.size * 3000 / t_train
+            xi = np.repeat(x, max(1, 1_000_000 // max(1, len(x))), axis=0)
+            CM.predict(xi[:1024])
+            t1 = time.perf_counter()
+            CM.predict(xi)
+            out["costmodel_infer_rows_per_s"] = len(xi) / (time.perf_counter() - t1)
+            out["costmodel_train_rows"] = int(y.size)
+            out["costmodel_train_mse"] = loss
+            out["costmodel_collect_train_s"] = time.perf_counter() - t0
+            held = W.random_mix_circuit(32, 16, seed=777)
+            big = lq.Statevector(32)
+            res = {}
+            for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED)):
+                prog = lq.simulator.CompiledCircuit(held, True, 0, mode)
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
+                prog.apply(big)
+                e.record()
+                torch.cuda.synchronize()
+                res[name] = (s.elapsed_time(e), prog.n_ops)
+            out["costmodel_32q_greedy_ms"] = res["greedy"][0]
+            out["costmodel_32q_learned_ms"] = res["learned"][0]
+            out["costmodel_32q_ops"] = {"greedy": res["greedy"][1], "learned": res["learned"][1]}
+            out["costmodel_32q_speedup"] = res["greedy"][0] / res["learned"][0]
+            del big
+            torch.cuda.empty_cache()
+        except Exception as ex:  # noqa: BLE001
+            out["costmodel_error"] = str(ex)
 
     # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets per call, the
     # default resident count: as many sets as keep their states in L2, 32 here): the first
     # call builds the plan and captures its CUDA graph, the timed call replays it with new
     # parameters; against direct launches, the plain one-set-at-a-time adjoint and the
     # reference's parameter-shift method run on the GPU
-    try:
-        pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
-        ham = W.random_hamiltonian(16, 500, seed=12)
-        sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
-        sets2 = W.random_parameter_sets(pc.num_parameters(), 256, seed=14)
-        lq.algorithms.adjoint_gradient(ham, pc, sets)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        lq.algorithms.adjoint_gradient(ham, pc, sets2)
-        t_b = time.perf_counter() - t0
-        os.environ["LQCS_GRAPHS"] = "0"
+    if want("adjoint"):
         try:
-            lq.algorithms.adjoint_gradient(ham, pc, sets[:1], max_resident=1)
+            pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+            ham = W.random_hamiltonian(16, 500, seed=12)
+            sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
+            sets2 = W.random_parameter_sets(pc.num_parameters(), 256, seed=14)
+            lq.algorithms.adjoint_gradient(ham, pc, sets)
+            torch.cuda.synchronize()
             t0 = time.perf_counter()
             lq.algorithms.adjoint_gradient(ham, pc, sets2)
-            t_d = time.perf_counter() - t0
+            t_b = time.perf_counter() - t0
+            os.environ["LQCS_GRAPHS"] = "0"
+            try:
+                lq.algorithms.adjoint_gradient(ham, pc, sets[:1], max_resident=1)
+                t0 = time.perf_counter()
+                lq.algorithms.adjoint_gradient(ham, pc, sets2)
+                t_d = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                for b in range(16):
+                    lq.algorithms.adjoint_gradient(ham, pc, sets[b], max_resident=1)
+                t_p = (time.perf_counter() - t0) / 16
+            finally:
+                os.environ.pop("LQCS_GRAPHS", None)
             t0 = time.perf_counter()
-            for b in range(16):
-                lq.algorithms.adjoint_gradient(ham, pc, sets[b], max_resident=1)
-            t_p = (time.perf_counter() - t0) / 16
-        finally:
-            os.environ.pop("LQCS_GRAPHS", None)
-        t0 = time.perf_counter()
-        lq.algorithms.parameter_shift_gradient(ham, pc, sets[0])
-        t_s = time.perf_counter() - t0
-        out["adjoint_batched_grads_per_s"] = 256 / t_b
-        out["adjoint_batched_direct_grads_per_s"] = 256 / t_d
-        out["adjoint_graph_speedup"] = t_d / t_b
-        out["adjoint_plain_grads_per_s"] = 1 / t_p
-        out["adjoint_speedup_vs_plain"] = (256 / t_b) * t_p
-        out["parameter_shift_gpu_grads_per_s"] = 1 / t_s
-        out["adjoint_speedup_vs_parameter_shift"] = (256 / t_b) * t_s
-    except Exception as ex:  # noqa: BLE001
-        out["adjoint_error"] = str(ex)
+            lq.algorithms.parameter_shift_gradient(ham, pc, sets[0])
+            t_s = time.perf_counter() - t0
+            out["adjoint_batched_grads_per_s"] = 256 / t_b
+            out["adjoint_batched_direct_grads_per_s"] = 256 / t_d
+            out["adjoint_graph_speedup"] = t_d / t_b
+            out["adjoint_plain_grads_per_s"] = 1 / t_p
+            out["adjoint_speedup_vs_plain"] = (256 / t_b) * t_p
+            out["parameter_shift_gpu_grads_per_s"] = 1 / t_s
+            out["adjoint_speedup_vs_parameter_shift"] = (256 / t_b) * t_s
+        except Exception as ex:  # noqa: BLE001
+            out["adjoint_error"] = str(ex)
     return out
 
 
