@@ -23,7 +23,7 @@ namespace lqcs_b200 {
 
 namespace {
 
-constexpr int kMmaThreads = 256;   // 8 warps
+constexpr int kMmaThreads = 512;   // 16 warps
 constexpr int kMmaGroups = 64;     // groups per CTA tile: one n-tile of 8 per warp
 
 void check_launch(const char* what) {
@@ -46,17 +46,15 @@ struct PDenseMma {
     uint32_t fixed[kMaxQubits];   // sorted controls and targets
 };
 
-// Row strides (in doubles) of the shared operands: = 4 (mod 16), so the 16 lanes of a
-// half-warp reading an 8-byte fragment element (row = lane % 4 or lane / 4, column = the
-// other) fall on 16 different 8-byte bank pairs.
-template <int K> __host__ __device__ constexpr int mat_stride() { return (2 << K) + 4; }
+// X (the gathered groups) in shared memory as double2 [member][group], row stride kXStride
+// double2: a B fragment (real row 4 ks + lane % 4 = member, re / im; column = group) reads
+// two rows of 16 consecutive doubles, one wavefront each.  Two buffers: the next tile's
+// groups arrive by cp.async while this tile computes.
 constexpr int kXStride = kMmaGroups + 4;
 
 template <int K>
 constexpr size_t mma_smem_bytes() {
-    return sizeof(double) * (static_cast<size_t>(2 << K) * mat_stride<K>() +
-                             static_cast<size_t>(2 << K) * kXStride) +
-           sizeof(uint64_t) * ((1u << K) + kMaxQubits + kMmaGroups);
+    return sizeof(double2) * 2 * static_cast<size_t>(1 << K) * kXStride;
 }
 
 __device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
@@ -65,77 +63,122 @@ __device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// Element (row, col) of the real embedding of the complex matrix m (D x D).
+template <int D>
+__device__ __forceinline__ double embedded(const double2* __restrict__ m, int row, int col) {
+    const double2 z = __ldg(m + (row >> 1) * D + (col >> 1));
+    const int a = row & 1, b = col & 1;
+    return a == b ? z.x : (a == 0 ? -z.y : z.y);
+}
+
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src, uint32_t src_bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem_src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Work split of the R/8 m-tiles and the 8 n-tiles (of 8 groups) over the 16 warps: each warp
+// keeps the A fragments of its m-tile in registers for the whole launch (the matrix is the
+// same for every tile) and reads the B fragments of its NPW n-tiles from shared memory.
 template <int K>
-__global__ void __launch_bounds__(kMmaThreads) k_dense_mma(double2* __restrict__ st, PDenseMma<K> p) {
+struct MmaSplit {
+    static constexpr int R = 2 << K;
+    static constexpr int MT = R / 8;                          // m-tiles (<= warps)
+    static constexpr int WARPS = kMmaThreads / 32;
+    static constexpr int NSPLIT = WARPS / MT;                 // warps sharing an m-tile
+    static constexpr int NPW = 8 / NSPLIT;                    // n-tiles per warp
+    static constexpr int KS = R / 4;                          // k-steps
+    static_assert(MT <= WARPS && WARPS % MT == 0 && 8 % NSPLIT == 0, "m-tile split");
+};
+
+// A thread's group within a tile (g = tid % 64) and members l = tid / 64 + 8 r: one group
+// base per tile, computed by the thread itself.
+template <int K>
+__device__ __forceinline__ uint64_t group_base(uint64_t g, const PDenseMma<K>& p) {
+    for (uint32_t i = 0; i < p.n_fixed; ++i) g = insert_zero_bit(g, p.fixed[i]);
+    return g | p.cmask;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kMmaThreads, 1) k_dense_mma(double2* __restrict__ st, PDenseMma<K> p) {
+    using S = MmaSplit<K>;
     constexpr int D = 1 << K;
-    constexpr int R = 2 * D;          // real rows / columns of the embedded matrix
-    constexpr int MT = R / 8;         // m-tiles
-    constexpr int SM = mat_stride<K>();
-    extern __shared__ __align__(16) double smd[];
-    double* Ms = smd;                         // R x SM
-    double* Xs = Ms + R * SM;                 // R x kXStride, then the results
-    uint64_t* soff = reinterpret_cast<uint64_t*>(Xs + R * kXStride);
-    uint64_t* sfix = soff + D;
-    uint64_t* sbase = sfix + kMaxQubits;      // this tile's group bases
-    for (int i = threadIdx.x; i < D * D; i += kMmaThreads) {
-        const int r = i / D, c = i % D;
-        const double2 m = p.mat[i];
-        Ms[(2 * r) * SM + 2 * c] = m.x;
-        Ms[(2 * r) * SM + 2 * c + 1] = -m.y;
-        Ms[(2 * r + 1) * SM + 2 * c] = m.y;
-        Ms[(2 * r + 1) * SM + 2 * c + 1] = m.x;
-    }
-    for (int i = threadIdx.x; i < D; i += kMmaThreads) soff[i] = p.off[i];
-    for (uint32_t i = threadIdx.x; i < p.n_fixed; i += kMmaThreads) sfix[i] = p.fixed[i];
-    __syncthreads();
-    const uint32_t nf = p.n_fixed;
-    double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
+    constexpr int MPT = D * kMmaGroups / kMmaThreads;         // members per thread
+    extern __shared__ __align__(16) double2 xs[];             // 2 buffers of D x kXStride
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = warp % S::MT, nset = warp / S::MT;
+    const int g_t = threadIdx.x % kMmaGroups, l_t = threadIdx.x / kMmaGroups;
+    double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
     const uint64_t n_tiles = (p.n_groups + kMmaGroups - 1) / kMmaGroups;
-    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const uint64_t g0 = tile * kMmaGroups;
-        if (threadIdx.x < kMmaGroups) {
-            uint64_t g = g0 + threadIdx.x;
-            for (uint32_t i = 0; i < nf; ++i) g = insert_zero_bit(g, static_cast<unsigned>(sfix[i]));
-            sbase[threadIdx.x] = g | p.cmask;
-        }
-        __syncthreads();
-        // gather: consecutive threads take consecutive groups of one member
-        for (int i = threadIdx.x; i < kMmaGroups * D; i += kMmaThreads) {
-            const int g = i % kMmaGroups, l = i / kMmaGroups;
-            double2 a = make_double2(0.0, 0.0);
-            if (g0 + g < p.n_groups) a = __ldcs(s + (sbase[g] | soff[l]));
-            Xs[(2 * l) * kXStride + g] = a.x;
-            Xs[(2 * l + 1) * kXStride + g] = a.y;
-        }
-        __syncthreads();
-        double acc[MT][2];
+
+    auto gather = [&](uint64_t tile, int buf) {
+        const uint64_t g = tile * kMmaGroups + g_t;
+        const bool ok = g < p.n_groups;
+        const uint64_t base = ok ? group_base<K>(g, p) : 0;
+        double2* x = xs + buf * D * kXStride;
 #pragma unroll
-        for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
-        const int ncol = 8 * warp + (lane >> 2);
-#pragma unroll 2
-        for (int kk = 0; kk < R; kk += 4) {
-            const double b = Xs[(kk + (lane & 3)) * kXStride + ncol];
+        for (int r = 0; r < MPT; ++r) {
+            const int l = l_t + r * (kMmaThreads / kMmaGroups);
+            cp_async16(x + l * kXStride + g_t, ok ? s + (base | p.off[l]) : s, ok ? 16u : 0u);
+        }
+    };
+
+    if (blockIdx.x < n_tiles) gather(blockIdx.x, 0);
+    cp_async_commit();
+    // A fragments: row 8 mt + lane / 4, column 4 ks + lane % 4 of the embedded matrix
+    double af[S::KS];
 #pragma unroll
-            for (int mt = 0; mt < MT; ++mt)
-                mma_f64(acc[mt], Ms[(8 * mt + (lane >> 2)) * SM + kk + (lane & 3)], b);
+    for (int ks = 0; ks < S::KS; ++ks) af[ks] = embedded<D>(p.mat, 8 * mt + (lane >> 2), 4 * ks + (lane & 3));
+
+    int buf = 0;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, buf ^= 1) {
+        if (tile + gridDim.x < n_tiles) gather(tile + gridDim.x, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait_prev();   // this tile's copies (all but the newest group) have landed
+        __syncthreads();
+        double2* x = xs + buf * D * kXStride;
+        const double* xd = reinterpret_cast<const double*>(x);
+        double acc[S::NPW][2];
+#pragma unroll
+        for (int j = 0; j < S::NPW; ++j) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < S::KS; ++ks) {
+            const int k = 4 * ks + (lane & 3);   // real row: member k / 2, re / im k % 2
+#pragma unroll
+            for (int j = 0; j < S::NPW; ++j) {
+                const int n = 8 * (nset * S::NPW + j) + (lane >> 2);
+                mma_f64(acc[j], af[ks], xd[((k >> 1) * kXStride + n) * 2 + (k & 1)]);
+            }
         }
         __syncthreads();   // every warp has read X: the results may overwrite it
+        {
+            double* xo = reinterpret_cast<double*>(x);
+            const int k = 8 * mt + (lane >> 2);
 #pragma unroll
-        for (int mt = 0; mt < MT; ++mt) {
-            double* row = Xs + (8 * mt + (lane >> 2)) * kXStride + 8 * warp + 2 * (lane & 3);
-            row[0] = acc[mt][0];
-            row[1] = acc[mt][1];
+            for (int j = 0; j < S::NPW; ++j) {
+                const int n = 8 * (nset * S::NPW + j) + 2 * (lane & 3);
+                xo[((k >> 1) * kXStride + n) * 2 + (k & 1)] = acc[j][0];
+                xo[((k >> 1) * kXStride + n + 1) * 2 + (k & 1)] = acc[j][1];
+            }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < kMmaGroups * D; i += kMmaThreads) {
-            const int g = i % kMmaGroups, l = i / kMmaGroups;
-            if (g0 + g < p.n_groups)
-                __stcs(s + (sbase[g] | soff[l]),
-                       make_double2(Xs[(2 * l) * kXStride + g], Xs[(2 * l + 1) * kXStride + g]));
+        {
+            const uint64_t g = tile * kMmaGroups + g_t;
+            if (g < p.n_groups) {
+                const uint64_t base = group_base<K>(g, p);
+#pragma unroll
+                for (int r = 0; r < MPT; ++r) {
+                    const int l = l_t + r * (kMmaThreads / kMmaGroups);
+                    __stcs(s + (base | p.off[l]), x[l * kXStride + g_t]);
+                }
+            }
         }
-        __syncthreads();
+        __syncthreads();   // the store has read this buffer: the gather after next may refill it
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 template <int K>
@@ -162,8 +205,7 @@ void mma_impl(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
     if (e != cudaSuccess)
         throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     const uint64_t tiles = (p.n_groups + kMmaGroups - 1) / kMmaGroups;
-    const uint32_t per_sm = static_cast<uint32_t>(std::max<size_t>(1, (227 * 1024) / (smem + 1024)));
-    const uint64_t want = static_cast<uint64_t>(ctx.num_sms) * std::min<uint32_t>(per_sm, 4);
+    const uint64_t want = static_cast<uint64_t>(ctx.num_sms);   // one 16-warp CTA per SM
     const uint32_t grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, tiles)));
     k_dense_mma<K><<<dim3(grid, batch), kMmaThreads, smem, ctx.stream>>>(st, p);
     check_launch("dense_mma");

@@ -366,11 +366,12 @@ def test_errors_match_reference_types():
 
 @pytest.mark.parametrize("width", [4, 5, 6])
 @pytest.mark.parametrize("mma", ["1", "0"])
-def test_wide_blocks_dmma_and_ffma(port, monkeypatch, width, mma):
+@pytest.mark.parametrize("n", [7, 14])
+def test_wide_blocks_dmma_and_ffma(port, monkeypatch, width, mma, n):
     """Greedy 4..6-qubit blocks (controls included) on the FP64 tensor path
-    (mma.sync.m8n8k4.f64) and on the FFMA kernel agree with the oracle."""
+    (mma.sync.m8n8k4.f64, 64 groups per tile: partial tiles at 7 qubits) and on the FFMA
+    kernel agree with the oracle."""
     monkeypatch.setenv("LQCS_DENSE_MMA", mma)
-    n = 14
     init = W.gaussian_state(n, seed=width)
     qc = random_circuit(n, 80, seed=100 + width, max_controls=3, max_unitary=4)
     want = port.run_statevector(qc, fuse=False, state=init)
