@@ -54,6 +54,11 @@ bool is_identity_scaled(const Kraus& m) {
            std::abs(m[3] - cd{1, 0}) < tol;
 }
 
+int env_int_or(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+
 bool use_fused(uint32_t n) {
     if (n < kRegMinBits) return false;
     const char* e = std::getenv("LQCS_TRAJ_FUSED");
@@ -127,10 +132,42 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
     auto st = new_state(n, R, cs);
     const LaunchCtx ctx = st->ctx;
 
+    // Shot order.  A general channel's event cuts the batch's gate stream only where some
+    // state's uniform is at or above the certainty bound, and then it cuts it for every state
+    // of the batch.  Shots whose events are all certain ("clean") therefore run together in
+    // batches of R without cuts; the others run in small batches that cut only where their
+    // own few states need it.  Batch position p holds shot order[p]; the device sees the
+    // uniforms in that order, and the registers go back to shot order at the end.
+    std::vector<uint64_t> order;
+    uint64_t n_clean = 0;
+    {
+        std::vector<char> dirty(f.shots, 0);
+        for (const Item& it : f.items) {
+            if (it.kind != kKrausGeneral) continue;
+            const double bound = lam[it.channel] - 1e-12;
+            for (uint64_t sh = 0; sh < f.shots; ++sh)
+                dirty[sh] |= f.u[sh * f.K + it.uidx] < bound ? 0 : 1;
+        }
+        order.reserve(f.shots);
+        for (uint64_t sh = 0; sh < f.shots; ++sh)
+            if (!dirty[sh]) order.push_back(sh);
+        n_clean = order.size();
+        for (uint64_t sh = 0; sh < f.shots; ++sh)
+            if (dirty[sh]) order.push_back(sh);
+    }
+    const uint32_t R_dirty = std::max<uint32_t>(1, std::min<uint32_t>(
+        R, static_cast<uint32_t>(env_int_or("LQCS_TRAJ_DIRTY_BATCH", 4))));
+    std::vector<double> u_perm(f.u.size());
+    for (uint64_t p = 0; p < f.shots; ++p)
+        std::copy(f.u.begin() + order[p] * f.K, f.u.begin() + (order[p] + 1) * f.K,
+                  u_perm.begin() + p * f.K);
+    std::vector<uint64_t> regs_perm(f.shots);
+
     DeviceBuffer d_u, part, mats, flag, scale, dregs;
-    d_u.ensure(sizeof(double) * std::max<size_t>(1, f.u.size()));
-    if (!f.u.empty())
-        cuda_check(cudaMemcpy(d_u.ptr, f.u.data(), sizeof(double) * f.u.size(), cudaMemcpyHostToDevice),
+    d_u.ensure(sizeof(double) * std::max<size_t>(1, u_perm.size()));
+    if (!u_perm.empty())
+        cuda_check(cudaMemcpy(d_u.ptr, u_perm.data(), sizeof(double) * u_perm.size(),
+                              cudaMemcpyHostToDevice),
                    "H2D uniforms");
     part.ensure(sizeof(double) * R * 4 * kTrajMaxBlocks);
     mats.ensure(sizeof(double2) * R * 4);
@@ -153,8 +190,11 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
     DeviceBuffer d_vals;
     d_vals.ensure(sizeof(uint64_t) * R);
 
-    for (uint64_t first = 0; first < f.shots; first += R) {
-        const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(R, f.shots - first));
+    for (uint64_t first = 0; first < f.shots;) {   // first: batch start position in `order`
+        const uint32_t nb = static_cast<uint32_t>(
+            first < n_clean ? std::min<uint64_t>(R, n_clean - first)
+                            : std::min<uint64_t>(R_dirty, f.shots - first));
+        auto shot = [&](uint32_t b) { return order[first + b]; };
         launch_set_basis(ctx, st->d(), n, nb, 0);
         cuda_check(cudaMemsetAsync(dregs.ptr, 0, sizeof(uint64_t) * nb, cs), "memset");
         cuda_check(cudaMemsetAsync(d_vals.ptr, 0, sizeof(uint64_t) * nb, cs), "memset");
@@ -213,11 +253,11 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
                     break;
                 case kKrausTable: {
                     const std::vector<int>& ch = f.choice[i];
-                    const int c0 = ch[first];
+                    const int c0 = ch[shot(0)];
                     bool any = false, same = true;
                     for (uint32_t b = 0; b < nb; ++b) {
-                        any |= ch[first + b] >= 0;
-                        same &= ch[first + b] == c0;
+                        any |= ch[shot(b)] >= 0;
+                        same &= ch[shot(b)] == c0;
                     }
                     if (!any) break;
                     if (same) {
@@ -228,7 +268,7 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
                     g.slot = true;
                     g.slot_id = static_cast<uint32_t>(slots[0].size());
                     for (uint32_t b = 0; b < nb; ++b) {
-                        const int c = ch[first + b];
+                        const int c = ch[shot(b)];
                         slots[b].push_back(c < 0 ? ident : f.norm[it.channel][c]);
                     }
                     seg.push_back(std::move(g));
@@ -239,7 +279,7 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
                     std::vector<int> forced(nb);
                     bool all = true;
                     for (uint32_t b = 0; b < nb; ++b) {
-                        forced[b] = f.u[(first + b) * f.K + it.uidx] < bound ? 0 : -1;
+                        forced[b] = f.u[shot(b) * f.K + it.uidx] < bound ? 0 : -1;
                         all &= forced[b] == 0;
                     }
                     if (all) {
@@ -289,10 +329,12 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
             }
         }
         flush();
-        cuda_check(cudaMemcpyAsync(regs + first, dregs.ptr, sizeof(uint64_t) * nb,
+        cuda_check(cudaMemcpyAsync(regs_perm.data() + first, dregs.ptr, sizeof(uint64_t) * nb,
                                    cudaMemcpyDeviceToHost, cs), "D2H registers");
         cuda_check(cudaStreamSynchronize(cs), "trajectory batch");
+        first += nb;
     }
+    for (uint64_t p = 0; p < f.shots; ++p) regs[order[p]] = regs_perm[p];
 }
 
 }  // namespace
