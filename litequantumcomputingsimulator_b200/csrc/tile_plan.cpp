@@ -403,13 +403,12 @@ static void merge_diagonal_runs(std::vector<LocalOp>& ops, uint32_t max_bits, bo
 // next op touching its qubit — or, failing that, the previous one — when that op is a dense
 // block on it without controls (the ops in between do not touch the qubit, so they commute
 // with it): the block's matrix absorbs it at no extra cost per amplitude and one operation
-// disappears.
+// disappears.  A noise slot (per-state matrix) folds too: the block becomes per-state.
 static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select) {
     std::vector<char> dead(ops.size(), 0);
     for (size_t i = 0; i < ops.size(); ++i) {
         LocalOp& p = ops[i];
-        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || p.variant ||
-            !p.dyn.empty())
+        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || !p.dyn.empty())
             continue;
         const uint32_t a = p.lt[0];
         for (size_t j = i + 1; j < ops.size(); ++j) {
@@ -419,13 +418,14 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
                                  std::find(q.lt.begin(), q.lt.end(), a) != q.lt.end();
             if (!touches) continue;
             const auto it = std::find(q.lt.begin(), q.lt.end(), a);
-            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask && !q.variant) {
+            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask) {
                 std::vector<uint32_t> sel = q.sel;
                 for (uint32_t s : p.sel)
                     if (std::find(sel.begin(), sel.end(), s) == sel.end()) sel.push_back(s);
                 std::sort(sel.begin(), sel.end());
                 if (sel.size() <= max_select || (p.sel.empty() && q.sel.size() <= max_select)) {
                     fold_into(q, p, static_cast<uint32_t>(it - q.lt.begin()), sel);
+                    q.variant = q.variant || p.variant;
                     dead[i] = 1;
                 }
             }
@@ -439,13 +439,14 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
                                  std::find(q.lt.begin(), q.lt.end(), a) != q.lt.end();
             if (!touches) continue;
             const auto it = std::find(q.lt.begin(), q.lt.end(), a);
-            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask && !q.variant) {
+            if (q.kind == kTileDense && it != q.lt.end() && !q.lmask && !q.gcmask) {
                 std::vector<uint32_t> sel = q.sel;
                 for (uint32_t s : p.sel)
                     if (std::find(sel.begin(), sel.end(), s) == sel.end()) sel.push_back(s);
                 std::sort(sel.begin(), sel.end());
                 if (sel.size() <= max_select || (p.sel.empty() && q.sel.size() <= max_select)) {
                     fold_into(q, p, static_cast<uint32_t>(it - q.lt.begin()), sel, true);
+                    q.variant = q.variant || p.variant;
                     dead[i] = 1;
                 }
             }
