@@ -407,7 +407,17 @@ static void merge_diagonal_runs(std::vector<LocalOp>& ops, uint32_t max_bits, bo
 static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select) {
     std::vector<char> dead(ops.size(), 0);
     for (size_t i = 0; i < ops.size(); ++i) {
-        LocalOp& p = ops[i];
+        // a phase on one tile bit (such as K0 of amplitude damping) folds as the diagonal
+        // (1, f); if it does not fold it keeps its phase form
+        LocalOp as_diag;
+        const bool one_bit_phase = ops[i].kind == kTilePhase && !ops[i].gcmask &&
+                                   ops[i].sel.empty() && __builtin_popcount(ops[i].lmask) == 1;
+        if (one_bit_phase) {
+            as_diag.kind = kTileDiag;
+            as_diag.lt = {static_cast<uint32_t>(__builtin_ctz(ops[i].lmask))};
+            as_diag.m = {cd{1, 0}, ops[i].m[0]};
+        }
+        const LocalOp& p = one_bit_phase ? as_diag : ops[i];
         if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || !p.dyn.empty())
             continue;
         const uint32_t a = p.lt[0];
@@ -633,8 +643,10 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
         open.push_back(std::move(nb));
     }
     for (Open& b : open) emit_block(b);
-    merge_diagonal_runs(out, max_diag, dyn_terms);
+    // one-qubit ops first go into the dense blocks on their qubits (free); the diagonal
+    // work left over then merges into tables
     fold_single_qubit_ops(out, max_select);
+    merge_diagonal_runs(out, max_diag, dyn_terms);
     return out;
 }
 
