@@ -709,8 +709,8 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
         except Exception as ex:  # noqa: BLE001
             out["costmodel_error"] = str(ex)
 
-    # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets per call, the
-    # default resident count: as many sets as keep their states in L2, 32 here): the first
+    # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets per call, all
+    # resident — the default resident count): the first
     # call builds the plan and captures its CUDA graph, the timed call replays it with new
     # parameters; against direct launches, the plain one-set-at-a-time adjoint and the
     # reference's parameter-shift method run on the GPU

@@ -132,33 +132,23 @@ void HamiltonianDev::upload(const Hamiltonian& h, uint32_t n) {
 
 namespace {
 
-// Resident sets per launch batch.  Every launch of a batch walks all its states (two per
-// set), so a batch whose states fit in about 60 % of L2 runs each launch from L2 instead of
-// HBM; it stays large enough to fill the GPU (2^20 amplitudes a launch).  At 16 qubits this
-// picks 32 sets (64 MiB): 3900 gradients/s against 2790 with 256 resident.
+// Resident sets per launch batch: as many as fit (two states per set), at most 256.  With
+// the rotation tile passes a launch is compute-heavy and larger batches amortise it better
+// (16 qubits: 7960 gradients/s with 256 sets, 7570 with 32).  One launch per step (fixed
+// gates, LQCS_ADJ_TILES=0) streams every state per step, and there a batch that stays in L2
+// is faster (32 sets: 4230 against 3210) — max_resident picks that size.
 uint32_t default_resident(uint32_t n, uint64_t batch) {
     size_t free_b = 0, total_b = 0;
     cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    int dev = 0, l2 = 0;
-    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-    cuda_check(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "L2 size");
     const uint64_t per_set = 2 * (uint64_t{16} << n);
     const uint64_t fit = std::max<uint64_t>(1, (free_b / 2) / per_set);
-    uint64_t in_l2 = 1;
-    while (2 * in_l2 * per_set <= static_cast<uint64_t>(l2) * 6 / 10) in_l2 *= 2;
-    const uint64_t fill = std::max<uint64_t>(1, (uint64_t{1} << 20) >> std::min<uint32_t>(n, 20));
-    return static_cast<uint32_t>(std::min<uint64_t>({batch, fit, 256, std::max(in_l2, fill)}));
+    return static_cast<uint32_t>(std::min<uint64_t>({batch, fit, 256}));
 }
 
 }  // namespace
 
 namespace {
 
-// Everything one (circuit, Hamiltonian, resident batch) needs on the device, kept between
-// calls: the fixed gates and their inverses, the two resident state batches, the Hamiltonian
-// terms and the per-set buffers, on a stream of its own.  A call only uploads the new
-// (cos, sin) tables, so the launch sequence of a batch of nb sets never changes: it is
-// captured once as a CUDA graph and replayed (LQCS_GRAPHS=0: launched directly).
 // One launch of the forward or backward sweep: a rotation tile pass (step < 0; its ops at
 // op_off in d_rot_ops) or one step launched on its own.
 struct Segment {
@@ -167,9 +157,8 @@ struct Segment {
     uint32_t op_off = 0;
 };
 
-// Greedy rotation tile passes over a run of parameterised steps, in the order given: a
-// rotation joins the open pass while the X bits above L of its rotations fit the m - L free
-// tile slots; a rotation whose own X bits do not fit runs on its own.
+// Rotation tile passes over a run of parameterised steps: a pass takes rotations while the
+// X bits above L of its rotations fit the m - L free tile slots.
 void plan_rotation_passes(const std::vector<const GateStep*>& run,
                           const std::vector<size_t>& index, uint32_t n, uint32_t m, uint32_t L,
                           std::vector<Segment>& segs, std::vector<RotTileOp>& all_ops) {
@@ -217,22 +206,40 @@ void plan_rotation_passes(const std::vector<const GateStep*>& run,
         cur.clear();
         H = 0;
     };
-    for (size_t r = 0; r < run.size(); ++r) {
-        const uint64_t need = run[r]->gen.x & ~low;
-        if (static_cast<uint32_t>(__builtin_popcountll(need)) > slots) {
-            close();
+    // Passes fill greedily over the pending rotations in order; a rotation may join ahead of
+    // rotations left for a later pass when it commutes with every one of them (Pauli strings
+    // commute when they anticommute on an even number of qubits), so the pass sequence is
+    // one factorisation of the same product.  A rotation too wide for a tile runs on its own.
+    auto commute = [](const PauliMasks& a, const PauliMasks& b) {
+        return ((__builtin_popcountll(a.x & b.zy) + __builtin_popcountll(a.zy & b.x)) & 1) == 0;
+    };
+    std::vector<size_t> pend(run.size());
+    for (size_t r = 0; r < run.size(); ++r) pend[r] = r;
+    while (!pend.empty()) {
+        const size_t f0 = pend.front();
+        if (static_cast<uint32_t>(__builtin_popcountll(run[f0]->gen.x & ~low)) > slots) {
             Segment own;
-            own.step = static_cast<int>(index[r]);
+            own.step = static_cast<int>(index[f0]);
             segs.push_back(own);
+            pend.erase(pend.begin());
             continue;
         }
-        if (!cur.empty() && (static_cast<uint32_t>(__builtin_popcountll(H | need)) > slots ||
-                             cur.size() == kRotMaxOps))
-            close();
-        H |= need;
-        cur.push_back(run[r]);
+        std::vector<size_t> rest;
+        for (size_t r : pend) {
+            const uint64_t need = run[r]->gen.x & ~low;
+            bool ok = static_cast<uint32_t>(__builtin_popcountll(H | need)) <= slots &&
+                      cur.size() < kRotMaxOps;
+            for (size_t k = 0; ok && k < rest.size(); ++k) ok = commute(run[r]->gen, run[rest[k]]->gen);
+            if (ok) {
+                H |= need;
+                cur.push_back(run[r]);
+            } else {
+                rest.push_back(r);
+            }
+        }
+        close();
+        pend = std::move(rest);
     }
-    close();
 }
 
 int env_or(const char* name, int dflt) {
@@ -240,6 +247,11 @@ int env_or(const char* name, int dflt) {
     return e ? std::atoi(e) : dflt;
 }
 
+// Everything one (circuit, Hamiltonian, resident batch) needs on the device, kept between
+// calls: the fixed gates and their inverses, the two resident state batches, the Hamiltonian
+// terms and the per-set buffers, on a stream of its own.  A call only uploads the new
+// (cos, sin) tables, so the launch sequence of a batch of nb sets never changes: it is
+// captured once as a CUDA graph and replayed (LQCS_GRAPHS=0: launched directly).
 struct AdjointPlan {
     uint64_t key = 0;
     uint32_t n = 0, R = 0;
