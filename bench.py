@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
     ap.add_argument("--extras", default=None,
                     help="comma-separated extra legs to run (sweep, unfused, qft, trajectories, "
-                         "width6, autotune, ragged, dm, costmodel, adjoint); default all")
+                         "width6, autotune, ragged, dm, costmodel, kernels, adjoint); default all")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -708,6 +708,62 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             torch.cuda.empty_cache()
         except Exception as ex:  # noqa: BLE001
             out["costmodel_error"] = str(ex)
+
+    # primitive kernels one gate (or reduction) at a time on the bench state, unfused: the
+    # gate kernels (1q at the lowest and highest target, controlled, phase, 2q dense, 2q
+    # diagonal, swap, Toffoli, Pauli rotations with and without X bits) timed with CUDA
+    # events over 3 launches, GB/s from the algorithmic bytes (32 B per amplitude the gate can
+    # change); the reductions (norm, Pauli expectation, 4096-shot sampling: prefix sum and
+    # search, collapse) host-timed around the call, GB/s from one 16 B read per amplitude
+    if want("kernels"):
+        try:
+            q = np.linalg.qr(np.random.default_rng(5).normal(size=(4, 4)) +
+                             1j * np.random.default_rng(6).normal(size=(4, 4)))[0]
+            cases = [
+                ("u3_t0", lambda c: c.u(0.3, 0.5, 0.7, 0)),
+                ("u3_t_top", lambda c: c.u(0.3, 0.5, 0.7, n - 1)),
+                ("cx", lambda c: c.cx(3, n - 2)),
+                ("cp", lambda c: c.cp(0.3, 2, n - 3)),
+                ("unitary_2q", lambda c: c.unitary(q, [1, n - 4])),
+                ("rzz", lambda c: c.rzz(0.4, 5, n - 5)),
+                ("swap", lambda c: c.swap(4, n - 6)),
+                ("ccx", lambda c: c.ccx(0, n - 1, 6)),
+                ("rp_XYZ", lambda c: c.rp(0.4, "XYZ", [0, 7, n - 1])),
+                ("rp_ZZ", lambda c: c.rp(0.4, "ZZ", [2, n - 2])),
+            ]
+            kern = {}
+            for name, add in cases:
+                c = lq.QuantumCircuit(n)
+                add(c)
+                pk = lq.simulator.CompiledCircuit(c, fuse_gates=False)
+                pk.apply(sv)
+                torch.cuda.synchronize()
+                s.record()
+                for _ in range(3):
+                    pk.apply(sv)
+                e.record()
+                torch.cuda.synchronize()
+                ms = s.elapsed_time(e) / 3
+                kern[name] = {"ms": round(ms, 3), "gbs": round(W.alg_bytes(c) / (ms / 1e3) / 1e9, 1)}
+            read_bytes = 16.0 * (1 << n)
+            pauli = "XZ" + "I" * (n - 4) + "YZ"
+            uni = np.random.default_rng(7).random(4096)
+            reductions = [("norm", lambda: sv.norm()),
+                          ("expectation_XZ..YZ", lambda: sv.expectation_value(pauli)),
+                          ("sample_4096", lambda: sv.sample(uni)),
+                          ("collapse", lambda: sv.collapse(n - 1, 0.25))]
+            for name, fn in reductions:
+                fn()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(3):
+                    fn()
+                ms = (time.perf_counter() - t0) / 3 * 1e3
+                kern[name] = {"ms": round(ms, 3), "gbs": round(read_bytes / (ms / 1e3) / 1e9, 1)}
+            out["kernels"] = kern
+            out["kernels_hbm_peak_gbs"] = hbm_peak
+        except Exception as ex:  # noqa: BLE001
+            out["kernels_error"] = str(ex)
 
     # batched adjoint gradients (16 qubits, 200 rp gates, 500 terms, 256 sets per call, all
     # resident — the default resident count): the first

@@ -126,10 +126,10 @@ void dm_run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& ga
     auto rho = dm_evolve(n, gates, opts);
     Rng rng = make_rng(opts);
     const uint64_t len = uint64_t{1} << n;
-    DeviceBuffer cum, seg, du, didx, dmargin;
-    cum.ensure(sizeof(double) * len);
+    DeviceBuffer tpref, seg, du, didx, dmargin;
+    tpref.ensure(sizeof(double) * scan_thread_count(n));
     seg.ensure(sizeof(double) * (scan_block_count(n) + 1));
-    launch_dm_diag_scan(rho->ctx, rho->d(), n, cum.as<double>(), seg.as<double>());
+    launch_dm_diag_scan(rho->ctx, rho->d(), n, tpref.as<double>(), seg.as<double>());
     std::vector<double> u(shots);
     if (opts && opts->shot_offset) rng.discard(opts->shot_offset);   // one uniform per shot
     for (uint64_t s = 0; s < shots; ++s) u[s] = rng_uniform(rng);
@@ -139,8 +139,8 @@ void dm_run_shots(uint32_t n, uint32_t n_clbits, const std::vector<GateDesc>& ga
     cuda_check(cudaMemcpyAsync(du.ptr, u.data(), sizeof(double) * shots, cudaMemcpyHostToDevice,
                                rho->stream),
                "H2D uniforms");
-    launch_sample_search(rho->ctx, cum.as<double>(), n, du.as<double>(), shots,
-                         didx.as<uint64_t>(), dmargin.as<double>());
+    launch_dm_sample_search(rho->ctx, rho->d(), n, tpref.as<double>(), seg.as<double>(),
+                            du.as<double>(), shots, didx.as<uint64_t>(), dmargin.as<double>());
     std::vector<uint64_t> idx(shots);
     cuda_check(cudaMemcpyAsync(idx.data(), didx.ptr, sizeof(uint64_t) * shots,
                                cudaMemcpyDeviceToHost, rho->stream),

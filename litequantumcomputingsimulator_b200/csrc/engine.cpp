@@ -729,10 +729,10 @@ double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k)
 
 void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin) {
     const uint64_t len = st.len();
-    DeviceBuffer cum, seg, du, didx, dmargin;
-    cum.ensure(sizeof(double) * len);
+    DeviceBuffer tpref, seg, du, didx, dmargin;
+    tpref.ensure(sizeof(double) * scan_thread_count(st.n));
     seg.ensure(sizeof(double) * (scan_block_count(st.n) + 1));
-    launch_prob_scan(st.ctx, st.d(), st.n, cum.as<double>(), seg.as<double>());
+    launch_prob_scan(st.ctx, st.d(), st.n, tpref.as<double>(), seg.as<double>());
     if (shots == 0) {
         if (min_margin) *min_margin = 1.0;
         st.sync();
@@ -744,8 +744,8 @@ void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, doub
     cuda_check(cudaMemcpyAsync(du.ptr, u, sizeof(double) * shots, cudaMemcpyHostToDevice,
                                st.stream),
                "H2D uniforms");
-    launch_sample_search(st.ctx, cum.as<double>(), st.n, du.as<double>(), shots,
-                         didx.as<uint64_t>(), dmargin.as<double>());
+    launch_sample_search(st.ctx, st.d(), st.n, tpref.as<double>(), seg.as<double>(),
+                         du.as<double>(), shots, didx.as<uint64_t>(), dmargin.as<double>());
     cuda_check(cudaMemcpyAsync(idx, didx.ptr, sizeof(uint64_t) * shots, cudaMemcpyDeviceToHost,
                                st.stream),
                "D2H sample indices");

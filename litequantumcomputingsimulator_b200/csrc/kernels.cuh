@@ -112,20 +112,26 @@ void launch_expect_xgroup(const LaunchCtx& ctx, const double2* st, uint32_t n, u
 // probabilities p[i] = |a_i|^2 (rounded like std::norm)
 void launch_probabilities(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_p);
 
-// Inclusive prefix sum of |a_i|^2 into d_cum (2^n doubles); d_block is scratch of
-// scan_block_count(n) doubles.
+// Sampling by inclusive prefix sum of |a_i|^2 and upper_bound per shot.  The scan stores
+// per-chunk prefixes in d_tpref (scan_thread_count(n) doubles) and per-segment prefixes in
+// d_block (scan_block_count(n) doubles); the search evaluates prefix values from them and the
+// state, so the 2^n-entry prefix array is never materialised.
 uint64_t scan_block_count(uint32_t n);
-void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_cum,
+uint64_t scan_thread_count(uint32_t n);
+void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_tpref,
                       double* d_block);
+// upper_bound(cum, u_s * cum[N-1]) per shot; d_margin[s] = distance to the nearest edge / total
+void launch_sample_search(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                          const double* d_tpref, const double* d_block, const double* d_u,
+                          uint64_t shots, uint64_t* d_idx, double* d_margin);
 // The same over the diagonal rho_ii of an n-qubit density matrix held as a 2n-qubit vector
 // (element (col << n) | row), and the diagonal itself (2^n doubles).
-void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_cum,
+void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_tpref,
                          double* d_block);
+void launch_dm_sample_search(const LaunchCtx& ctx, const double2* rho, uint32_t n,
+                             const double* d_tpref, const double* d_block, const double* d_u,
+                             uint64_t shots, uint64_t* d_idx, double* d_margin);
 void launch_dm_diagonal(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_p);
-// upper_bound(cum, u_s * cum[N-1]) per shot; d_margin[s] = distance to the nearest edge / total
-void launch_sample_search(const LaunchCtx& ctx, const double* d_cum, uint32_t n,
-                          const double* d_u, uint64_t shots, uint64_t* d_idx,
-                          double* d_margin);
 
 // collapse: amplitudes with bit q == outcome scaled by `scale`, the others zeroed
 void launch_project(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t q, int outcome,

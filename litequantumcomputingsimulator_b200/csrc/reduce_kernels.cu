@@ -209,18 +209,34 @@ __global__ void __launch_bounds__(kReduceThreads) k_expect(const double2* __rest
 #pragma unroll
     for (int k = 0; k < static_cast<int>(2 * kMaxTermsPerPass); ++k) v[k] = 0.0;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.len;
-         i += stride) {
-        const double2 a = __ldg(s + i), b = __ldg(s + (i ^ p.x));
-        // a * conj(b)
-        const double wr = a.x * b.x + a.y * b.y;
-        const double wi = a.y * b.x - a.x * b.y;
+    if (p.x == 0) {
+        for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+             i < p.len; i += stride) {
+            const double2 a = __ldg(s + i);
+            const double wr = a.x * a.x + a.y * a.y;
 #pragma unroll
-        for (int t = 0; t < static_cast<int>(kMaxTermsPerPass); ++t) {
-            if (t < static_cast<int>(p.n_terms)) {
-                const double sg = parity_sign(i & p.zy[t]);
-                v[2 * t] += sg * wr;
-                v[2 * t + 1] += sg * wi;
+            for (int t = 0; t < static_cast<int>(kMaxTermsPerPass); ++t) {
+                if (t < static_cast<int>(p.n_terms)) v[2 * t] += parity_sign(i & p.zy[t]) * wr;
+            }
+        }
+    } else {
+        // each pair (i, i ^ x) once: the term at i ^ x is the conjugate of the one at i, with
+        // its own sign, so every amplitude is read once
+        const unsigned hb = 63u - static_cast<unsigned>(__clzll(p.x));
+        for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+             g < p.len / 2; g += stride) {
+            const uint64_t i = insert_zero_bit(g, hb), j = i ^ p.x;
+            const double2 a = __ldg(s + i), b = __ldg(s + j);
+            // a * conj(b) at i; b * conj(a) = its conjugate at j
+            const double wr = a.x * b.x + a.y * b.y;
+            const double wi = a.y * b.x - a.x * b.y;
+#pragma unroll
+            for (int t = 0; t < static_cast<int>(kMaxTermsPerPass); ++t) {
+                if (t < static_cast<int>(p.n_terms)) {
+                    const double si = parity_sign(i & p.zy[t]), sj = parity_sign(j & p.zy[t]);
+                    v[2 * t] += (si + sj) * wr;
+                    v[2 * t + 1] += (si - sj) * wi;
+                }
             }
         }
     }
@@ -291,6 +307,12 @@ void launch_probabilities(const LaunchCtx& ctx, const double2* st, uint32_t n, d
 // amplitudes), thread totals are combined by a sequential scan in fixed order, and the
 // segment prefixes are added at the end.  The result differs from the sequential sum only
 // in rounding; lqcs_state_sample reports how far each shot was from a bin edge.
+//
+// The prefix array itself is never stored: the scan keeps each thread chunk's exclusive
+// prefix within its segment (tpref, one double per 16 amplitudes) and the segments'
+// exclusive prefixes (block), and the search evaluates an element of the prefix array when
+// its binary search probes it — re-adding at most 16 probabilities in the scan's own order,
+// so every probed value is the one the full array would hold.
 constexpr uint32_t kScanThreads = 256;
 constexpr uint32_t kPerThread = 16;
 constexpr uint64_t kSegAmps = uint64_t{kScanThreads} * kPerThread;
@@ -299,6 +321,8 @@ uint64_t scan_block_count(uint32_t n) {
     const uint64_t len = uint64_t{1} << n;
     return (len + kSegAmps - 1) / kSegAmps;
 }
+
+uint64_t scan_thread_count(uint32_t n) { return scan_block_count(n) * kScanThreads; }
 
 // Probability sources of the scan: |a_i|^2 of a statevector, or the diagonal rho_ii of a
 // density matrix stored as a 2n-qubit vector (element (col << n) | row).
@@ -314,38 +338,29 @@ struct DiagSource {
 
 template <class Src>
 __global__ void __launch_bounds__(kScanThreads) k_scan_seg(Src src, uint64_t len,
-                                                           double* __restrict__ cum,
+                                                           double* __restrict__ tpref_out,
                                                            double* __restrict__ seg_total) {
     __shared__ double tsum[kScanThreads];
     const uint64_t seg0 = static_cast<uint64_t>(blockIdx.x) * kSegAmps;
     const uint64_t i0 = seg0 + static_cast<uint64_t>(threadIdx.x) * kPerThread;
-    double local[kPerThread];
     double acc = 0.0;
 #pragma unroll
     for (uint32_t k = 0; k < kPerThread; ++k) {
         const uint64_t i = i0 + k;
         const double p = (i < len) ? src(i) : 0.0;
         acc = (k == 0) ? p : __dadd_rn(acc, p);
-        local[k] = acc;
     }
     tsum[threadIdx.x] = acc;
     __syncthreads();
-    // exclusive prefix of the thread totals, sequential in thread order (warp 0 does it)
-    __shared__ double tpref[kScanThreads];
+    // exclusive prefix of the thread totals, sequential in thread order
     if (threadIdx.x == 0) {
         double run = 0.0;
+        double* tp = tpref_out + static_cast<uint64_t>(blockIdx.x) * kScanThreads;
         for (uint32_t t = 0; t < kScanThreads; ++t) {
-            tpref[t] = run;
+            tp[t] = run;
             run = __dadd_rn(run, tsum[t]);
         }
         seg_total[blockIdx.x] = run;
-    }
-    __syncthreads();
-    const double off = tpref[threadIdx.x];
-#pragma unroll
-    for (uint32_t k = 0; k < kPerThread; ++k) {
-        const uint64_t i = i0 + k;
-        if (i < len) cum[i] = (threadIdx.x == 0) ? local[k] : __dadd_rn(off, local[k]);
     }
 }
 
@@ -381,41 +396,27 @@ __global__ void __launch_bounds__(1024) k_scan_top(double* __restrict__ seg, uin
     }
 }
 
-__global__ void k_scan_add(double* __restrict__ cum, uint64_t len,
-                           const double* __restrict__ seg_prefix) {
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < len;
-         i += stride) {
-        const uint64_t b = i / kSegAmps;
-        if (b > 0) cum[i] = __dadd_rn(seg_prefix[b], cum[i]);
-    }
-}
-
 template <class Src>
-void prob_scan(const LaunchCtx& ctx, Src src, uint32_t n, double* d_cum, double* d_block) {
+void prob_scan(const LaunchCtx& ctx, Src src, uint32_t n, double* d_tpref, double* d_block) {
     const uint64_t len = uint64_t{1} << n;
     const uint64_t nseg = scan_block_count(n);
-    k_scan_seg<Src><<<static_cast<uint32_t>(nseg), kScanThreads, 0, ctx.stream>>>(src, len, d_cum,
+    k_scan_seg<Src><<<static_cast<uint32_t>(nseg), kScanThreads, 0, ctx.stream>>>(src, len, d_tpref,
                                                                                   d_block);
     check_launch("scan_seg");
     if (nseg > 1) {
         k_scan_top<<<1, 1024, 0, ctx.stream>>>(d_block, nseg);
         check_launch("scan_top");
-        const uint32_t nb = static_cast<uint32_t>(std::min<uint64_t>(
-            (len + 255) / 256, static_cast<uint64_t>(ctx.num_sms) * 8));
-        k_scan_add<<<nb, 256, 0, ctx.stream>>>(d_cum, len, d_block);
-        check_launch("scan_add");
     }
 }
 
-void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_cum,
+void launch_prob_scan(const LaunchCtx& ctx, const double2* st, uint32_t n, double* d_tpref,
                       double* d_block) {
-    prob_scan(ctx, AmpSource{st}, n, d_cum, d_block);
+    prob_scan(ctx, AmpSource{st}, n, d_tpref, d_block);
 }
 
-void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_cum,
+void launch_dm_diag_scan(const LaunchCtx& ctx, const double2* rho, uint32_t n, double* d_tpref,
                          double* d_block) {
-    prob_scan(ctx, DiagSource{rho, n}, n, d_cum, d_block);
+    prob_scan(ctx, DiagSource{rho, n}, n, d_tpref, d_block);
 }
 
 __global__ void k_dm_diag(const double2* __restrict__ rho, uint32_t n, double* __restrict__ p) {
@@ -434,19 +435,37 @@ void launch_dm_diagonal(const LaunchCtx& ctx, const double2* rho, uint32_t n, do
     check_launch("dm_diag");
 }
 
+// Element j of the inclusive prefix array, evaluated as the scan would have stored it:
+// the thread chunk's running sum up to j, plus the chunk's prefix in its segment (not for
+// the first chunk), plus the segment's prefix (not for the first segment, and only when
+// there is more than one).
+template <class Src>
+__device__ double cum_at(const Src& src, uint64_t j, const double* __restrict__ tpref,
+                         const double* __restrict__ seg_prefix, uint64_t nseg) {
+    const uint64_t b = j / kSegAmps;
+    const uint32_t t = static_cast<uint32_t>((j % kSegAmps) / kPerThread);
+    const uint64_t i0 = b * kSegAmps + static_cast<uint64_t>(t) * kPerThread;
+    double local = src(i0);
+    for (uint64_t i = i0 + 1; i <= j; ++i) local = __dadd_rn(local, src(i));
+    const double c = (t == 0) ? local : __dadd_rn(tpref[b * kScanThreads + t], local);
+    return (b > 0 && nseg > 1) ? __dadd_rn(seg_prefix[b], c) : c;
+}
+
 // std::upper_bound(cum, cum + N, u * total) for every shot
-// (src/backend/statevector_simulator.cpp:105-109).
-__global__ void k_sample_search(const double* __restrict__ cum, uint64_t len,
+// (src/backend/statevector_simulator.cpp:105-109), probing cum through cum_at.
+template <class Src>
+__global__ void k_sample_search(Src src, uint64_t len, const double* __restrict__ tpref,
+                                const double* __restrict__ seg_prefix, uint64_t nseg,
                                 const double* __restrict__ u, uint64_t shots,
                                 uint64_t* __restrict__ idx, double* __restrict__ margin) {
     const uint64_t s = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (s >= shots) return;
-    const double total = cum[len - 1];
+    const double total = cum_at(src, len - 1, tpref, seg_prefix, nseg);
     const double r = u[s] * total;
     uint64_t lo = 0, count = len;
     while (count > 0) {
         const uint64_t half = count >> 1;
-        if (!(r < cum[lo + half])) {
+        if (!(r < cum_at(src, lo + half, tpref, seg_prefix, nseg))) {
             lo = lo + half + 1;
             count = count - half - 1;
         } else {
@@ -455,20 +474,35 @@ __global__ void k_sample_search(const double* __restrict__ cum, uint64_t len,
     }
     idx[s] = lo;
     if (margin) {
-        const double below = (lo > 0) ? cum[lo - 1] : 0.0;
-        const double above = (lo < len) ? cum[lo] : total;
+        const double below = (lo > 0) ? cum_at(src, lo - 1, tpref, seg_prefix, nseg) : 0.0;
+        const double above = (lo < len) ? cum_at(src, lo, tpref, seg_prefix, nseg) : total;
         margin[s] = fmin(r - below, above - r) / total;
     }
 }
 
-void launch_sample_search(const LaunchCtx& ctx, const double* d_cum, uint32_t n,
-                          const double* d_u, uint64_t shots, uint64_t* d_idx,
-                          double* d_margin) {
+template <class Src>
+void sample_search(const LaunchCtx& ctx, Src src, uint32_t n, const double* d_tpref,
+                   const double* d_block, const double* d_u, uint64_t shots, uint64_t* d_idx,
+                   double* d_margin) {
     if (shots == 0) return;
     const uint64_t len = uint64_t{1} << n;
-    const uint32_t nb = static_cast<uint32_t>((shots + 255) / 256);
-    k_sample_search<<<nb, 256, 0, ctx.stream>>>(d_cum, len, d_u, shots, d_idx, d_margin);
+    const uint32_t nb = static_cast<uint32_t>((shots + 127) / 128);
+    k_sample_search<Src><<<nb, 128, 0, ctx.stream>>>(src, len, d_tpref, d_block,
+                                                     scan_block_count(n), d_u, shots, d_idx,
+                                                     d_margin);
     check_launch("sample_search");
+}
+
+void launch_sample_search(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                          const double* d_tpref, const double* d_block, const double* d_u,
+                          uint64_t shots, uint64_t* d_idx, double* d_margin) {
+    sample_search(ctx, AmpSource{st}, n, d_tpref, d_block, d_u, shots, d_idx, d_margin);
+}
+
+void launch_dm_sample_search(const LaunchCtx& ctx, const double2* rho, uint32_t n,
+                             const double* d_tpref, const double* d_block, const double* d_u,
+                             uint64_t shots, uint64_t* d_idx, double* d_margin) {
+    sample_search(ctx, DiagSource{rho, n}, n, d_tpref, d_block, d_u, shots, d_idx, d_margin);
 }
 
 // ---------------------------------------------------------------- projection
