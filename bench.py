@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
     ap.add_argument("--extras", default=None,
                     help="comma-separated extra legs to run (sweep, unfused, qft, trajectories, "
-                         "width6, autotune, ragged, dm, costmodel, kernels, adjoint); default all")
+                         "width6, autotune, ragged, dm, costmodel, config0, kernels, adjoint); default all")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -692,7 +692,7 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             held = W.random_mix_circuit(32, 16, seed=777)
             big = lq.Statevector(32)
             res = {}
-            for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED)):
+            for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED), ("default", 0)):
                 prog = lq.simulator.CompiledCircuit(held, True, 0, mode)
                 s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s.record()
@@ -702,12 +702,35 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
                 res[name] = (s.elapsed_time(e), prog.n_ops)
             out["costmodel_32q_greedy_ms"] = res["greedy"][0]
             out["costmodel_32q_learned_ms"] = res["learned"][0]
-            out["costmodel_32q_ops"] = {"greedy": res["greedy"][1], "learned": res["learned"][1]}
+            out["costmodel_32q_default_ms"] = res["default"][0]
+            out["costmodel_32q_ops"] = {k: v[1] for k, v in res.items()}
             out["costmodel_32q_speedup"] = res["greedy"][0] / res["learned"][0]
             del big
             torch.cuda.empty_cache()
         except Exception as ex:  # noqa: BLE001
             out["costmodel_error"] = str(ex)
+
+    # the 20-qubit workload (brickwork depth 20, measure_all, 4096 shots under a fixed seed)
+    # through StatevectorSimulator.run, and the smallest distance of any shot's uniform from
+    # a bin edge of the prefix sum (relative to the total): what keeps the counts identical
+    # to those of the reference's sequential sum
+    if want("config0"):
+        try:
+            q0 = W.brickwork(20, 20, seed=2024, measure=True)
+            sim0 = lq.StatevectorSimulator(seed=42)
+            sim0.run(q0, 4096)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sim0.run(q0, 4096)
+            dt = time.perf_counter() - t0
+            n_gates = sum(1 for ins in q0.instructions() if ins.gate.is_unitary())
+            sv0 = lq.StatevectorSimulator(seed=42).run_statevector(W.brickwork(20, 20, seed=2024))
+            _, margin0 = sv0.sample(W.UniformStream(42).take(4096))
+            out["config0_run_ms"] = dt * 1e3
+            out["config0_gates_per_s"] = n_gates / dt
+            out["config0_min_margin"] = margin0
+        except Exception as ex:  # noqa: BLE001
+            out["config0_error"] = str(ex)
 
     # primitive kernels one gate (or reduction) at a time on the bench state, unfused: the
     # gate kernels (1q at the lowest and highest target, controlled, phase, 2q dense, 2q
