@@ -668,13 +668,15 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["dm_error"] = str(ex)
 
     # learned fusion cost model: trained on the engine's own per-operation timings of
-    # random-mix circuits (24-26 qubits, all candidate plans), then the learned plan and the
-    # greedy plan of a held-out 32-qubit circuit (64 GiB state) are timed on the device
+    # random-mix circuits (24-30 qubits, all candidate plans), then the learned plan, the
+    # greedy plan and the default plan of a held-out 32-qubit circuit (64 GiB state) are
+    # timed on the device
     if want("costmodel"):
         try:
             from litequantumcomputingsimulator_b200 import costmodel as CM
             train_set = [W.random_mix_circuit(nq, d, s) for nq, d, s in
-                         [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14)]]
+                         [(24, 12, 11), (25, 10, 12), (26, 8, 13), (24, 20, 14), (28, 8, 15),
+                          (30, 6, 16)]]
             t0 = time.perf_counter()
             x, y = CM.collect(train_set)
             t1 = time.perf_counter()

@@ -409,17 +409,19 @@ int lqcs_autotune(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_i
 /* ------------------------------------------------------------------ cost model
  * A 3-layer, 64-wide FP32 MLP predicting the device time of one device operation from
  * LQCS_COST_FEATURES features (op kind, width, lowest / highest qubit touched, source gate
- * count, register size; see lqcs_costmodel_features), trained by the engine's own FP32
+ * count, register size, FP64 flops per amplitude; see lqcs_costmodel_features), trained by
+ * the engine's own FP32
  * forward / backward / Adam kernels on timings the engine measures
  * (lqcs_program_apply_profiled).  fusion_mode 2 uses it to choose among candidate fusion
  * plans; without trained weights it falls back to the greedy plan.  Engine extension: no
  * counterpart in the reference.  Targets are log(milliseconds per 2^24 amplitudes). */
-enum { LQCS_COST_FEATURES = 6, LQCS_COST_HIDDEN = 64 };
+enum { LQCS_COST_FEATURES = 7, LQCS_COST_HIDDEN = 64 };
 
-/* Feature row of one operation (kind as in lqcs_op_profile). */
+/* Feature row of one operation (kind as in lqcs_op_profile; flops_per_amp = its alg_flops
+ * divided by the amplitudes of one state). */
 int lqcs_costmodel_features(uint32_t kind, uint32_t width, uint32_t min_target,
                             uint32_t max_target, uint32_t n_gates, uint32_t n_qubits,
-                            float* out);
+                            double flops_per_amp, float* out);
 
 /* Train from scratch on n rows (features n x LQCS_COST_FEATURES, targets n); the weights
  * stay in the library.  loss_out (may be NULL) receives the final mean squared error. */

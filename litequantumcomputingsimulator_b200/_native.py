@@ -174,7 +174,7 @@ SIGNATURES = {
     "lqcs_dm_run": (C.c_int, [C.c_uint32, C.c_uint32, _P(Instruction), C.c_uint64, C.c_uint64,
                               _P(SimOptions), C.c_void_p]),
     "lqcs_costmodel_features": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
-                                          C.c_uint32, C.c_uint32, C.c_void_p]),
+                                          C.c_uint32, C.c_uint32, C.c_double, C.c_void_p]),
     "lqcs_costmodel_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_float,
                                        C.c_uint64, _P(C.c_float)]),
     "lqcs_costmodel_predict": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),

@@ -3,7 +3,7 @@
 The model (a 3-layer, 64-wide FP32 MLP inside the engine library, trained by the engine's
 own kernels) predicts log(device milliseconds per 2^24 amplitudes) of one device
 operation from (op kind, width, lowest / highest qubit touched, source gate count,
-register size).  Training data are the engine's own per-operation timings: circuits are
+register size, FP64 flops per amplitude).  Training data are the engine's own per-operation timings: circuits are
 compiled under several candidate plans (greedy dense blocks of width 1..6, tile passes of
 several shapes) and applied once with CUDA-event timing per operation
 (``lqcs_program_apply_profiled``).  ``StatevectorSimulator(fusion_mode=2)`` then scores every
@@ -24,7 +24,7 @@ import numpy as np
 from . import _native as N
 from .simulator import CompiledCircuit, Statevector
 
-FEATURES = 6
+FEATURES = 7
 TILE_KIND = 6
 GREEDY, LEARNED, TILE = 1, 2, 4
 TILE_SHAPES = [(11, 5, 2), (12, 5, 2), (12, 5, 3), (13, 5, 2), (13, 5, 3)]
@@ -46,9 +46,11 @@ def tile_shape(m: int, low: int, inner: int):
                 os.environ[k] = v
 
 
-def features(kind: int, width: int, lo: int, hi: int, gates: int, n: int) -> np.ndarray:
+def features(kind: int, width: int, lo: int, hi: int, gates: int, n: int,
+             flops_per_amp: float = 0.0) -> np.ndarray:
     out = np.zeros(FEATURES, dtype=np.float32)
-    N.call("lqcs_costmodel_features", kind, width, lo, hi, gates, n, out.ctypes.data)
+    N.call("lqcs_costmodel_features", kind, width, lo, hi, gates, n, float(flops_per_amp),
+           out.ctypes.data)
     return out
 
 
@@ -62,7 +64,7 @@ def profile_rows(prog: CompiledCircuit, sv: Statevector, n: int):
     for r in prog.profile(sv):
         kind = r["kind"]
         lo, hi = r["min_target"], r["max_target"]
-        xs.append(features(kind, r["width"], lo, hi, r["gates"], n))
+        xs.append(features(kind, r["width"], lo, hi, r["gates"], n, r["alg_flops"] / float(1 << n)))
         ys.append(target_of(r["ms"], n))
     return xs, ys
 
@@ -82,7 +84,7 @@ def candidate_programs(circuit):
 
 
 def collect(circuits, warm: bool = True):
-    """Profile every candidate plan of every circuit: returns (X [rows, 6], y [rows])."""
+    """Profile every candidate plan of every circuit: returns (X [rows, FEATURES], y [rows])."""
     xs, ys = [], []
     for qc in circuits:
         n = qc.num_qubits()

@@ -448,10 +448,11 @@ int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonia
 
 int lqcs_costmodel_features(uint32_t kind, uint32_t width, uint32_t min_target,
                             uint32_t max_target, uint32_t n_gates, uint32_t n_qubits,
-                            float* out) {
+                            double flops_per_amp, float* out) {
     return guarded([&] {
         need(out, "out");
-        const auto f = lqcs_b200::op_features(kind, width, min_target, max_target, n_gates, n_qubits);
+        const auto f = lqcs_b200::op_features(kind, width, min_target, max_target, n_gates, n_qubits,
+                                              flops_per_amp);
         for (int i = 0; i < lqcs_b200::kCostFeatures; ++i) out[i] = f[i];
     });
 }

@@ -5,6 +5,7 @@
 // 2^24 amplitudes).  Parameters are one flat FP32 array: W1 [64][F], b1 [64], W2 [64][64],
 // b2 [64], W3 [64], b3 [1].  Every reduction over samples runs in a fixed order (one thread
 // per parameter looping over the samples), so training is deterministic.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <random>
@@ -317,10 +318,12 @@ void costmodel_set_weights(const float* w, uint64_t n) {
 }
 
 std::array<float, kCostFeatures> op_features(uint32_t kind, uint32_t width, uint32_t min_target,
-                                             uint32_t max_target, uint32_t gates, uint32_t n) {
+                                             uint32_t max_target, uint32_t gates, uint32_t n,
+                                             double flops_per_amp) {
     return {static_cast<float>(kind) / 6.0f, static_cast<float>(width) / 8.0f,
             static_cast<float>(min_target) / 32.0f, static_cast<float>(max_target) / 32.0f,
-            std::log2(1.0f + static_cast<float>(gates)) / 8.0f, static_cast<float>(n) / 32.0f};
+            std::log2(1.0f + static_cast<float>(gates)) / 8.0f, static_cast<float>(n) / 32.0f,
+            static_cast<float>(std::log2(1.0 + std::max(0.0, flops_per_amp))) / 10.0f};
 }
 
 std::array<float, kCostFeatures> op_features(const DevOp& op, uint32_t n) {
@@ -328,7 +331,7 @@ std::array<float, kCostFeatures> op_features(const DevOp& op, uint32_t n) {
     for (uint32_t t : op.targets) mask |= uint64_t{1} << t;
     const uint32_t lo = mask ? static_cast<uint32_t>(__builtin_ctzll(mask)) : 0;
     const uint32_t hi = mask ? 63u - static_cast<uint32_t>(__builtin_clzll(mask)) : 0;
-    return op_features(profile_kind(op), op.k, lo, hi, op.src_gates, n);
+    return op_features(profile_kind(op), op.k, lo, hi, op.src_gates, n, op_flops_per_amp(op));
 }
 
 double predict_ops_ms(const std::vector<DevOp>& ops, uint32_t n) {

@@ -10,14 +10,17 @@
 namespace lqcs_b200 {
 
 // Features of one device operation: op kind, width, lowest and highest qubit it touches,
-// number of source gates, register size.  Scaled to O(1) by op_features.
-constexpr int kCostFeatures = 6;
+// number of source gates, register size, FP64 flops per amplitude (for a tile pass the
+// flops of all its operations: what its time grows with beyond the one HBM round trip).
+// Scaled to O(1) by op_features.
+constexpr int kCostFeatures = 7;
 constexpr int kCostHidden = 64;
 constexpr int kCostParams = kCostHidden * kCostFeatures + kCostHidden +
                             kCostHidden * kCostHidden + kCostHidden + kCostHidden + 1;
 
 std::array<float, kCostFeatures> op_features(uint32_t kind, uint32_t width, uint32_t min_target,
-                                             uint32_t max_target, uint32_t gates, uint32_t n);
+                                             uint32_t max_target, uint32_t gates, uint32_t n,
+                                             double flops_per_amp);
 std::array<float, kCostFeatures> op_features(const DevOp& op, uint32_t n);
 
 // Train from scratch on (features, targets); returns the final mean squared error.

@@ -10,7 +10,7 @@ from litequantumcomputingsimulator_b200 import costmodel as CM
 from litequantumcomputingsimulator_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
-F, H = 6, 64
+F, H = CM.FEATURES, 64
 
 
 def unpack(w):
