@@ -298,7 +298,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     // per-tile diagonal tables, two sets (tile parity) on a 16-byte boundary
     double2* sdyn = reinterpret_cast<double2*>(
         (reinterpret_cast<uintptr_t>(slay + p.n_layouts) + 15u) & ~uintptr_t{15});
-    __shared__ uint64_t gbit[kRegMaxBits];   // global offset of each tile bit
+    __shared__ uint64_t gbit[kRegMaxBits];    // global offset of each tile bit at the load
+    __shared__ uint64_t sgbit[kRegMaxBits];   // and at the store (relabelled by SWAPs)
     __shared__ uint32_t shbits[kTileMaxHigh];
     __shared__ uint32_t sdynrec[kRegMaxDyn];
     if (threadIdx.x == 0) {
@@ -308,6 +309,9 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
         for (uint32_t i = 0; i < kRegMaxDyn; ++i) sdynrec[i] = p.dyn_rec[i];
         for (uint32_t b = 0; b < M; ++b)
             gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
+#pragma unroll
+        for (uint32_t b = 0; b < kRegMaxBits; ++b)
+            if (b < M) sgbit[b] = p.relabel ? uint64_t{1} << p.store_qubit[b] : gbit[b];
     }
     {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(
@@ -441,9 +445,9 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
         }
         {
             const RegLayout& ly = slay[cur];
-            const uint64_t g = base | thread_goff(ly, kTB, gbit);
-            const uint64_t g0 = gbit[ly.rpos[0]], g1 = gbit[ly.rpos[1]], g2 = gbit[ly.rpos[2]],
-                           g3 = gbit[ly.rpos[3]];
+            const uint64_t g = base | thread_goff(ly, kTB, sgbit);
+            const uint64_t g0 = sgbit[ly.rpos[0]], g1 = sgbit[ly.rpos[1]], g2 = sgbit[ly.rpos[2]],
+                           g3 = sgbit[ly.rpos[3]];
 #pragma unroll
             for (int u = 0; u < kE; ++u)
                 __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |

@@ -130,6 +130,8 @@ struct RegPass {
     uint32_t n_dyn;           // per-tile diagonals: their record indices and table entries
     uint32_t dyn_entries;
     uint8_t dyn_rec[kRegMaxDyn];
+    uint32_t relabel;         // SWAPs relabelled tile bits: tile bit b is stored to the place
+    uint8_t store_qubit[kRegMaxBits];   // of qubit store_qubit[b]
 };
 
 static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");

@@ -138,10 +138,30 @@ namespace {
 struct LocalMap {
     uint32_t L;
     std::vector<uint32_t> hbits;
-    int local(uint32_t q) const {   // -1 if outside the tile
+    // tile bit of qubit q, where a relabelling (virtual SWAP) has moved it; -1: none
+    std::vector<std::pair<uint32_t, uint32_t>> moved;
+    int home(uint32_t q) const {   // tile bit at load, -1 if outside the tile
         if (q < L) return static_cast<int>(q);
         const auto it = std::find(hbits.begin(), hbits.end(), q);
         return it == hbits.end() ? -1 : static_cast<int>(L + (it - hbits.begin()));
+    }
+    int local(uint32_t q) const {   // -1 if outside the tile
+        for (const auto& [qq, b] : moved)
+            if (qq == q) return static_cast<int>(b);
+        return home(q);
+    }
+    void swap_bits(uint32_t a, uint32_t b) {
+        const uint32_t la = static_cast<uint32_t>(local(a)), lb = static_cast<uint32_t>(local(b));
+        auto set = [&](uint32_t q, uint32_t bit) {
+            for (auto& e : moved)
+                if (e.first == q) {
+                    e.second = bit;
+                    return;
+                }
+            moved.emplace_back(q, bit);
+        };
+        set(a, lb);
+        set(b, la);
     }
 };
 
@@ -475,8 +495,9 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
                                     const TileConfig& cfg, uint32_t max_select,
                                     const std::vector<std::array<cd, 4>>* slot_mats,
-                                    uint32_t max_diag, bool dyn_terms) {
-    LocalMap lm{cfg.L, item.hbits};
+                                    uint32_t max_diag, bool dyn_terms,
+                                    std::vector<uint32_t>* store_qubits) {
+    LocalMap lm{cfg.L, item.hbits, {}};
     std::vector<LocalOp> out;
     // a noise slot takes this state's matrix (identity when no table is given)
     auto resolved = [&](const GateDesc& g) {
@@ -599,6 +620,15 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
 
     for (uint32_t gi : item.gates) {
         const GateDesc& g = gates[gi];
+        // a SWAP of two tile qubits moves no data: the two tile bits trade qubits for the rest
+        // of the pass, and the store writes each tile bit to its qubit's place
+        if (store_qubits && g.type == LQCS_GATE_SWAP && g.n_controls == 0 && !g.slot &&
+            g.qubits.size() == 2 && lm.local(g.qubits[0]) >= 0 && lm.local(g.qubits[1]) >= 0) {
+            for (uint32_t q : g.qubits)
+                if (owner[q] >= 0) emit_block(open[owner[q]]);
+            lm.swap_bits(g.qubits[0], g.qubits[1]);
+            continue;
+        }
         std::vector<uint32_t> part, sel;   // local qubits; out-of-tile controls
         for (uint32_t q : g.qubits) (lm.local(q) >= 0 ? part : sel).push_back(q);
         std::sort(part.begin(), part.end());
@@ -647,6 +677,14 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
     // work left over then merges into tables
     fold_single_qubit_ops(out, max_select);
     merge_diagonal_runs(out, max_diag, dyn_terms);
+    if (store_qubits) {   // qubit each tile bit holds at the end of the pass
+        const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
+        store_qubits->assign(m, 0);
+        for (uint32_t b = 0; b < m; ++b) {
+            const uint32_t q = b < cfg.L ? b : item.hbits[b - cfg.L];
+            (*store_qubits)[static_cast<uint32_t>(lm.local(q))] = q;
+        }
+    }
     return out;
 }
 
@@ -941,7 +979,9 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     const uint32_t m = cfg.L + static_cast<uint32_t>(item.hbits.size());
     const std::vector<std::array<cd, 4>>* slots0 =
         state_slots && !state_slots->empty() ? &(*state_slots)[0] : nullptr;
-    const std::vector<LocalOp> ops = pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true);
+    std::vector<uint32_t> store_q;
+    const std::vector<LocalOp> ops =
+        pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true, &store_q);
     for (const LocalOp& o : ops)
         if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : kRegMaxDiag))
             return false;
@@ -990,12 +1030,23 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             sync_tiles = true;
         }
     }
-    if (((S | W) & lanes) != 0) {   // the store wants lanes on tile bits 0..4 again
-        if ((W & lanes) == 0) {
-            seq.emplace_back(-1, layout_index(high & ~W, W));
+    // The store wants the lanes on the tile bits that hold qubits of tile bits 0..4 at the
+    // load (the same bits unless a relabelling moved those qubits).
+    uint32_t slanes = 0;
+    for (uint32_t l = 0; l < kLaneBits; ++l) {
+        const uint32_t q = l < cfg.L ? l : item.hbits[l - cfg.L];
+        for (uint32_t b = 0; b < m; ++b)
+            if (store_q[b] == q) slanes |= 1u << b;
+    }
+    const uint32_t shigh = all & ~slanes;
+    if (((S | W) & slanes) != 0) {
+        if ((W & slanes) == 0) {
+            seq.emplace_back(-1, layout_index(shigh & ~W, W));
         } else {
-            const uint32_t Sf = all & ~((1u << (m - kRegBits)) - 1u);
-            W = pick_warp_bits(ops, pending, high & ~Sf, nwarp);
+            uint32_t Sf = 0;   // the four highest tile bits outside the store lanes
+            for (int b = static_cast<int>(m) - 1; b >= 0 && __builtin_popcount(Sf) < static_cast<int>(kRegBits); --b)
+                if ((shigh >> b) & 1) Sf |= 1u << b;
+            W = pick_warp_bits(ops, pending, shigh & ~Sf, nwarp);
             seq.emplace_back(-2, layout_index(Sf, W));
             sync_tiles = true;
         }
@@ -1031,9 +1082,11 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     // every further state: same records, its own slot matrices
     if (state_slots) {
         for (size_t b = 1; b < state_slots->size(); ++b) {
-            const std::vector<LocalOp> ob =
-                pass_local_ops(item, gates, cfg, max_select, &(*state_slots)[b], kRegMaxDiag, true);
-            if (ob.size() != ops.size()) return false;
+            std::vector<uint32_t> store_b;
+            const std::vector<LocalOp> ob = pass_local_ops(item, gates, cfg, max_select,
+                                                           &(*state_slots)[b], kRegMaxDiag, true,
+                                                           &store_b);
+            if (ob.size() != ops.size() || store_b != store_q) return false;
             for (size_t i = 0; i < ops.size(); ++i)
                 if (!same_shape(ops[i], ob[i])) return false;
             const size_t before = mats.size();
@@ -1052,6 +1105,11 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     pass.n_mat = static_cast<uint32_t>(n_mat);
     pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
     pass.sync_tiles = sync_tiles ? 1u : 0u;
+    for (uint32_t b = 0; b < m; ++b) {
+        pass.store_qubit[b] = static_cast<uint8_t>(store_q[b]);
+        const uint32_t home = b < cfg.L ? b : item.hbits[b - cfg.L];
+        if (store_q[b] != home) pass.relabel = 1;
+    }
     pass.n_dyn = static_cast<uint32_t>(dyn_rec.size());
     pass.dyn_entries = dyn_entries;
     for (size_t d = 0; d < dyn_rec.size(); ++d) pass.dyn_rec[d] = static_cast<uint8_t>(dyn_rec[d]);

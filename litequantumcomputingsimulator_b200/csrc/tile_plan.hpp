@@ -54,11 +54,14 @@ struct LocalOp {
 // qubits outside the tile: those bits are constant over a tile, so the block becomes one
 // matrix per value of them, picked per tile.
 // Runs of commuting diagonal work merge into diagonals of at most max_diag tile bits; with
-// dyn_terms, phases gated by other out-of-tile qubits join them as per-tile terms.
+// dyn_terms, phases gated by other out-of-tile qubits join them as per-tile terms.  With
+// store_qubits, SWAPs of two tile qubits become relabellings (no operation) and
+// store_qubits[b] receives the qubit whose place tile bit b is stored to.
 std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<GateDesc>& gates,
                                     const TileConfig& cfg, uint32_t max_select,
                                     const std::vector<std::array<cd, 4>>* slot_mats = nullptr,
-                                    uint32_t max_diag = kTileMaxK, bool dyn_terms = false);
+                                    uint32_t max_diag = kTileMaxK, bool dyn_terms = false,
+                                    std::vector<uint32_t>* store_qubits = nullptr);
 
 // Append the tile operations of one pass to ops_out (matrices to arena) and fill `pass`.
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,

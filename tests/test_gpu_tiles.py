@@ -116,6 +116,32 @@ def test_diagonal_runs_and_gated_phases(port, tile_env, n, reg):
     assert np.max(np.abs(run(q, TILE, init) - want)) < TOL
 
 
+@pytest.mark.parametrize("n", [12, 15])
+def test_relabelled_swaps(port, tile_env, n):
+    """SWAPs of two tile qubits become relabellings in register passes (the store writes
+    each tile bit to its qubit's new place): chains of swaps between low and high qubits,
+    interleaved with dense and diagonal gates, and a full qubit reversal."""
+    tile_env(12, 5, 2, 1)
+    rng = np.random.default_rng(n)
+    qc = lq.QuantumCircuit(n)
+    for step in range(150):
+        a, b = (int(x) for x in rng.permutation(n)[:2])
+        k = int(rng.integers(5))
+        if k < 2:
+            qc.swap(a, b)
+        elif k == 2:
+            qc.u(*(float(x) for x in rng.uniform(0, 6.3, 3)), a)
+        elif k == 3:
+            qc.cx(a, b)
+        else:
+            qc.cp(float(rng.uniform(0, 6.3)), a, b)
+    for i in range(n // 2):
+        qc.swap(i, n - 1 - i)
+    init = W.gaussian_state(n, seed=n + 1)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+
+
 @pytest.mark.parametrize("reg", [1, 0])
 def test_tile_barrier_and_wide_gates(port, tile_env, reg):
     tile_env(12, 5, 2, reg)
