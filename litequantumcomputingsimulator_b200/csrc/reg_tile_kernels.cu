@@ -309,10 +309,13 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
         for (uint32_t i = 0; i < kRegMaxDyn; ++i) sdynrec[i] = p.dyn_rec[i];
         for (uint32_t b = 0; b < M; ++b)
             gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
+        if (p.relabel) {
 #pragma unroll
-        for (uint32_t b = 0; b < kRegMaxBits; ++b)
-            if (b < M) sgbit[b] = p.relabel ? uint64_t{1} << p.store_qubit[b] : gbit[b];
+            for (uint32_t b = 0; b < kRegMaxBits; ++b)
+                if (b < M) sgbit[b] = uint64_t{1} << p.store_qubit[b];
+        }
     }
+    const uint64_t* __restrict__ stbit = p.relabel ? sgbit : gbit;   // uniform
     {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(
             mats + static_cast<uint64_t>(blockIdx.y) * p.mat_stride);   // this state's matrices
@@ -445,9 +448,9 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
         }
         {
             const RegLayout& ly = slay[cur];
-            const uint64_t g = base | thread_goff(ly, kTB, sgbit);
-            const uint64_t g0 = sgbit[ly.rpos[0]], g1 = sgbit[ly.rpos[1]], g2 = sgbit[ly.rpos[2]],
-                           g3 = sgbit[ly.rpos[3]];
+            const uint64_t g = base | thread_goff(ly, kTB, stbit);
+            const uint64_t g0 = stbit[ly.rpos[0]], g1 = stbit[ly.rpos[1]], g2 = stbit[ly.rpos[2]],
+                           g3 = stbit[ly.rpos[3]];
 #pragma unroll
             for (int u = 0; u < kE; ++u)
                 __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
