@@ -81,6 +81,21 @@ def test_fused_explicit_kraus_counts_identical(ref, resident):
     assert got == want
 
 
+def test_fused_trajectories_with_swaps(ref):
+    """SWAPs between noisy layers (relabelled inside register passes, per-state noise
+    matrices in the same passes): counts equal the reference's per-shot semantics."""
+    qc = lq.QuantumCircuit(10, 10)
+    qc.compose(W.brickwork(10, 4, seed=9, noise=(0.05, 0.1, 0.2)))
+    for i in range(5):
+        qc.swap(i, 9 - i)
+    qc.swap(0, 3)
+    qc.compose(W.brickwork(10, 2, seed=10, noise=(0.05, 0.1, 0.2)))
+    qc.measure_all()
+    want = counts_of(ref.trajectories(qc, 96, 21))
+    got = counts_of(lq.StatevectorSimulator(seed=21, max_resident=32).run_registers(qc, 96))
+    assert got == want
+
+
 def test_fused_noise_model_counts_identical(ref):
     noise = lq.NoiseModel()
     noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.05))
