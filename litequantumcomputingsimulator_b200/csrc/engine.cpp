@@ -728,31 +728,29 @@ double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k)
 }
 
 void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin) {
-    const uint64_t len = st.len();
-    DeviceBuffer tpref, seg, du, didx, dmargin;
-    tpref.ensure(sizeof(double) * scan_thread_count(st.n));
-    seg.ensure(sizeof(double) * (scan_block_count(st.n) + 1));
-    launch_prob_scan(st.ctx, st.d(), st.n, tpref.as<double>(), seg.as<double>());
+    const uint64_t n_t = scan_thread_count(st.n), n_s = scan_block_count(st.n) + 1;
+    st.sample_scratch.ensure(sizeof(double) * (n_t + n_s + 3 * shots));
+    double* tpref = st.sample_scratch.as<double>();
+    double* seg = tpref + n_t;
+    double* du = seg + n_s;
+    uint64_t* didx = reinterpret_cast<uint64_t*>(du + shots);
+    double* dmargin = du + 2 * shots;
+    launch_prob_scan(st.ctx, st.d(), st.n, tpref, seg);
     if (shots == 0) {
         if (min_margin) *min_margin = 1.0;
         st.sync();
         return;
     }
-    du.ensure(sizeof(double) * shots);
-    didx.ensure(sizeof(uint64_t) * shots);
-    dmargin.ensure(sizeof(double) * shots);
-    cuda_check(cudaMemcpyAsync(du.ptr, u, sizeof(double) * shots, cudaMemcpyHostToDevice,
-                               st.stream),
+    cuda_check(cudaMemcpyAsync(du, u, sizeof(double) * shots, cudaMemcpyHostToDevice, st.stream),
                "H2D uniforms");
-    launch_sample_search(st.ctx, st.d(), st.n, tpref.as<double>(), seg.as<double>(),
-                         du.as<double>(), shots, didx.as<uint64_t>(), dmargin.as<double>());
-    cuda_check(cudaMemcpyAsync(idx, didx.ptr, sizeof(uint64_t) * shots, cudaMemcpyDeviceToHost,
+    launch_sample_search(st.ctx, st.d(), st.n, tpref, seg, du, shots, didx, dmargin);
+    cuda_check(cudaMemcpyAsync(idx, didx, sizeof(uint64_t) * shots, cudaMemcpyDeviceToHost,
                                st.stream),
                "D2H sample indices");
     std::vector<double> margins;
     if (min_margin) {
         margins.resize(shots);
-        cuda_check(cudaMemcpyAsync(margins.data(), dmargin.ptr, sizeof(double) * shots,
+        cuda_check(cudaMemcpyAsync(margins.data(), dmargin, sizeof(double) * shots,
                                    cudaMemcpyDeviceToHost, st.stream),
                    "D2H margins");
     }

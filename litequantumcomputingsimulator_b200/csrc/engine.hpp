@@ -123,6 +123,10 @@ struct lqcs_state {
     cudaStream_t stream = nullptr;
     lqcs_b200::DeviceBuffer amps;
     lqcs_b200::DeviceBuffer scratch;   // reductions (device)
+    // sampling: chunk and segment prefixes, uniforms, indices, margins — kept with the state
+    // (the largest request so far: 0.5 B per amplitude plus 24 B per shot), so repeated
+    // sampling allocates nothing
+    lqcs_b200::DeviceBuffer sample_scratch;
     lqcs_b200::LaunchCtx ctx;
 
     double2* d() const { return amps.as<double2>(); }

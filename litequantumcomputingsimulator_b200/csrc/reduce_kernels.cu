@@ -341,13 +341,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_seg(Src src, uint64_t len
                                                            double* __restrict__ tpref_out,
                                                            double* __restrict__ seg_total) {
     __shared__ double tsum[kScanThreads];
+    // the segment's probabilities, read coalesced; element e at e + e / kPerThread (one pad
+    // slot per chunk, so the chunk-wise reads below hit distinct banks)
+    __shared__ double sp[kSegAmps + kSegAmps / kPerThread];
     const uint64_t seg0 = static_cast<uint64_t>(blockIdx.x) * kSegAmps;
-    const uint64_t i0 = seg0 + static_cast<uint64_t>(threadIdx.x) * kPerThread;
+#pragma unroll
+    for (uint32_t k = 0; k < kPerThread; ++k) {
+        const uint32_t e = k * kScanThreads + threadIdx.x;
+        const uint64_t i = seg0 + e;
+        sp[e + e / kPerThread] = (i < len) ? src(i) : 0.0;
+    }
+    __syncthreads();
     double acc = 0.0;
 #pragma unroll
     for (uint32_t k = 0; k < kPerThread; ++k) {
-        const uint64_t i = i0 + k;
-        const double p = (i < len) ? src(i) : 0.0;
+        const double p = sp[threadIdx.x * (kPerThread + 1) + k];
         acc = (k == 0) ? p : __dadd_rn(acc, p);
     }
     tsum[threadIdx.x] = acc;
