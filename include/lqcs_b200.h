@@ -365,9 +365,10 @@ int lqcs_adjoint_gradient_multi(uint64_t n_problems, const lqcs_parametric_circu
                                 const uint64_t* batches, double* const* energy_out,
                                 double* const* grad_out);
 
-/* Frees what repeated gradient calls keep on the device between calls — the resident state
- * batches and captured graphs of the last adjoint plans — and the autotuner's choices.
- * Engine extension: no counterpart in the reference. */
+/* Frees what repeated calls keep on the device between calls — the resident state batches
+ * and captured graphs of the last adjoint plans, the compiled programs of the last 16
+ * circuits run (run / run_statevector reuse them for the same circuit and options) — and
+ * the autotuner's choices.  Engine extension: no counterpart in the reference. */
 int lqcs_release_caches(void);
 
 /* Energies only, batched (forward pass of lqcs_adjoint_gradient). */

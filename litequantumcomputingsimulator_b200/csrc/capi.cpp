@@ -432,6 +432,7 @@ int lqcs_release_caches(void) {
     return guarded([&] {
         lqcs_b200::release_adjoint_plans();
         lqcs_b200::clear_autotune_cache();
+        lqcs_b200::clear_program_cache();
     });
 }
 

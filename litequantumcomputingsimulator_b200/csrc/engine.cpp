@@ -4,6 +4,7 @@
 #include "costmodel.hpp"
 
 #include <algorithm>
+#include <deque>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -583,6 +584,82 @@ std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t s
     return st;
 }
 
+// Compiled programs of the most recent circuits, so that running the same circuit again
+// (a sampling loop, repeated run_statevector) skips planning and upload.  The key is the
+// whole gate list with every compile-time setting it depends on (device, register size,
+// fusion options, tile shape, environment overrides); learned and autotuned plans keep their
+// own caches and are compiled per call.
+namespace {
+
+std::mutex g_prog_mu;
+std::deque<std::pair<std::string, std::shared_ptr<const Program>>> g_progs;   // newest last
+constexpr size_t kProgramCache = 16;
+
+std::string program_key(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc) {
+    std::string k;
+    auto put = [&](const void* p, size_t len) { k.append(static_cast<const char*>(p), len); };
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    const TileConfig tc = default_tile_config(n);
+    const uint32_t fw = default_fusion_width();
+    const uint8_t tiles = use_tiles(n, fc) ? 1 : 0, fuse = fc.fuse ? 1 : 0, reg = tc.reg ? 1 : 0;
+    put(&dev, sizeof dev);
+    put(&n, sizeof n);
+    put(&fuse, 1);
+    put(&fc.mode, sizeof fc.mode);
+    put(&fc.max_width, sizeof fc.max_width);
+    put(&fw, sizeof fw);
+    put(&tiles, 1);
+    put(&tc.m, sizeof tc.m);
+    put(&tc.L, sizeof tc.L);
+    put(&tc.inner, sizeof tc.inner);
+    put(&reg, 1);
+    for (const GateDesc& g : gates) {
+        const uint64_t sizes[5] = {g.qubits.size(), g.params.size(), g.mat.size(), g.perm.size(),
+                                   g.pauli.size()};
+        put(&g.type, sizeof g.type);
+        put(&g.n_controls, sizeof g.n_controls);
+        put(sizes, sizeof sizes);
+        put(g.qubits.data(), g.qubits.size() * sizeof(uint32_t));
+        put(g.params.data(), g.params.size() * sizeof(double));
+        put(g.mat.data(), g.mat.size() * sizeof(cd));
+        put(g.perm.data(), g.perm.size() * sizeof(uint64_t));
+        put(g.pauli.data(), g.pauli.size());
+    }
+    return k;
+}
+
+std::shared_ptr<const Program> cached_program(const std::vector<GateDesc>& gates, uint32_t n,
+                                              const FusionConfig& fc, cudaStream_t stream) {
+    if (fc.fuse && (fc.mode == kFuseLearned || fc.mode == kFuseAutotune))
+        return std::make_shared<const Program>(compile(gates, n, fc, stream));
+    const std::string key = program_key(gates, n, fc);
+    {
+        std::lock_guard<std::mutex> lk(g_prog_mu);
+        for (auto it = g_progs.begin(); it != g_progs.end(); ++it) {
+            if (it->first == key) {
+                auto hit = *it;
+                g_progs.erase(it);
+                g_progs.push_back(hit);
+                return hit.second;
+            }
+        }
+    }
+    auto prog = std::make_shared<const Program>(compile(gates, n, fc, stream));
+    cuda_check(cudaStreamSynchronize(stream), "program upload");   // usable from any stream
+    std::lock_guard<std::mutex> lk(g_prog_mu);
+    g_progs.emplace_back(key, prog);
+    if (g_progs.size() > kProgramCache) g_progs.pop_front();
+    return prog;
+}
+
+}  // namespace
+
+void clear_program_cache() {
+    std::lock_guard<std::mutex> lk(g_prog_mu);
+    g_progs.clear();
+}
+
 void apply_circuit(lqcs_state& st, const std::vector<GateDesc>& gates, const FusionConfig& fc) {
     std::vector<GateDesc> keep;
     keep.reserve(gates.size());
@@ -595,8 +672,8 @@ void apply_circuit(lqcs_state& st, const std::vector<GateDesc>& gates, const Fus
         if (g.type == LQCS_GATE_MEASURE) continue;
         keep.push_back(g);
     }
-    Program p = compile(keep, st.n, fc, st.stream);
-    p.launch(st.ctx, st.d(), st.n, st.batch);
+    const std::shared_ptr<const Program> p = cached_program(keep, st.n, fc, st.stream);
+    p->launch(st.ctx, st.d(), st.n, st.batch);
     st.sync();
 }
 

@@ -99,6 +99,8 @@ struct TuneTiming {
 std::vector<TuneTiming> autotune(const std::vector<GateDesc>& gates, uint32_t n, size_t* best);
 void clear_autotune_cache();
 uint32_t default_fusion_width();
+// Drop the compiled programs kept for repeated circuits (apply_circuit).
+void clear_program_cache();
 
 // Compile a list of unitary gates to a Program (fused or gate by gate).
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,

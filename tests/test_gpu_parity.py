@@ -325,6 +325,28 @@ def test_adjoint_rotation_tile_passes(ref, monkeypatch, n):
     assert np.max(np.abs(g_t[2] - want)) < 1e-9
 
 
+def test_repeated_runs_reuse_compiled_programs(port, monkeypatch):
+    """run_statevector / run keep the compiled programs of recent circuits: a repeated call
+    gives the same amplitudes bit for bit, a changed tile setting compiles anew (and still
+    matches the oracle), and release_caches drops them without changing results."""
+    qc = W.brickwork(14, 6, seed=3)
+    want = port.run_statevector(qc, fuse=False)
+    sim = lq.StatevectorSimulator()
+    a = sim.run_statevector(qc).to_numpy()
+    b = sim.run_statevector(qc).to_numpy()
+    assert np.array_equal(a, b) and np.max(np.abs(a - want)) < TOL
+    monkeypatch.setenv("LQCS_TILE_BITS", "11")
+    c = sim.run_statevector(qc).to_numpy()
+    assert np.max(np.abs(c - want)) < TOL
+    monkeypatch.delenv("LQCS_TILE_BITS")
+    lq.algorithms.release_caches()
+    assert np.array_equal(sim.run_statevector(qc).to_numpy(), a)
+    m = W.brickwork(14, 6, seed=3, measure=True)
+    r1 = lq.StatevectorSimulator(seed=4).run_registers(m, 500)
+    r2 = lq.StatevectorSimulator(seed=4).run_registers(m, 500)
+    assert np.array_equal(r1, r2)
+
+
 def test_adjoint_batched_equals_single(ref):
     pc, _ = W.random_pauli_ansatz(8, 24, seed=8)
     h = W.random_hamiltonian(8, 40, seed=9)
