@@ -433,6 +433,7 @@ int lqcs_release_caches(void) {
         lqcs_b200::release_adjoint_plans();
         lqcs_b200::clear_autotune_cache();
         lqcs_b200::clear_program_cache();
+        lqcs_b200::clear_state_pool();
     });
 }
 

@@ -533,6 +533,8 @@ Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConf
 
 // ------------------------------------------------------------------ state handle
 
+lqcs_state::~lqcs_state() { lqcs_b200::pool_return(*this); }
+
 double* lqcs_state::partials(size_t values) {
     const size_t need = (lqcs_b200::kMaxReduceBlocks + 1) * values * 2 * sizeof(double) + 4096;
     scratch.ensure(need);
@@ -563,6 +565,84 @@ uint32_t max_qubits_on_device(uint32_t batch) {
     return q;
 }
 
+// Freed amplitude buffers of at most 1 GiB (a 26-qubit state), kept for the next state of the
+// same size on the same device: short runs (sampling loops, small circuits, trajectory
+// batches of small states) skip cudaMalloc and cudaFree, which synchronise the device.  At
+// most four buffers are kept; lqcs_release_caches frees them.
+namespace {
+
+struct PooledBuffer {
+    int device;
+    size_t bytes;
+    void* ptr;
+};
+// Never destroyed: states may be freed during process exit, after static destructors ran.
+std::mutex& pool_mu() {
+    static auto* m = new std::mutex;
+    return *m;
+}
+std::vector<PooledBuffer>& pool() {   // oldest first
+    static auto* p = new std::vector<PooledBuffer>;
+    return *p;
+}
+constexpr size_t kPoolMaxBytes = size_t{1} << 30;
+constexpr size_t kPoolEntries = 4;
+
+void* pool_take(int device, size_t bytes) {
+    std::lock_guard<std::mutex> lk(pool_mu());
+    for (auto it = pool().begin(); it != pool().end(); ++it) {
+        if (it->device == device && it->bytes == bytes) {
+            void* p = it->ptr;
+            pool().erase(it);
+            return p;
+        }
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+void clear_state_pool() {
+    std::vector<PooledBuffer> drop;
+    {
+        std::lock_guard<std::mutex> lk(pool_mu());
+        drop.swap(pool());
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (const PooledBuffer& b : drop) {
+        cudaSetDevice(b.device);
+        cudaFree(b.ptr);
+    }
+    cudaSetDevice(cur);
+}
+
+void pool_return(lqcs_state& st) {
+    if (!st.amps.ptr || st.amps.bytes > kPoolMaxBytes) return;
+    // the buffer is reused only after this state's work on it has finished
+    if (cudaStreamSynchronize(st.stream) != cudaSuccess) return;
+    void* evict = nullptr;
+    int evict_dev = 0;
+    {
+        std::lock_guard<std::mutex> lk(pool_mu());
+        if (pool().size() >= kPoolEntries) {
+            evict = pool().front().ptr;
+            evict_dev = pool().front().device;
+            pool().erase(pool().begin());
+        }
+        pool().push_back({st.device, st.amps.bytes, st.amps.ptr});
+    }
+    st.amps.ptr = nullptr;
+    st.amps.bytes = 0;
+    if (evict) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(evict_dev);
+        cudaFree(evict);
+        cudaSetDevice(cur);
+    }
+}
+
 std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t stream) {
     if (n == 0) invalid("Statevector: num_qubits must be >= 1");
     if (batch == 0) invalid("state batch must be >= 1");
@@ -579,7 +659,13 @@ std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t s
     st->batch = batch;
     st->stream = stream;
     st->ctx = make_ctx(stream);
-    st->amps.ensure(sizeof(double2) * st->len() * batch);
+    const size_t bytes = sizeof(double2) * st->len() * batch;
+    if (void* p = pool_take(st->device, bytes)) {
+        st->amps.ptr = p;
+        st->amps.bytes = bytes;
+    } else {
+        st->amps.ensure(bytes);
+    }
     launch_set_basis(st->ctx, st->d(), n, batch, 0);
     return st;
 }
@@ -591,8 +677,15 @@ std::unique_ptr<lqcs_state> new_state(uint32_t n, uint32_t batch, cudaStream_t s
 // own caches and are compiled per call.
 namespace {
 
-std::mutex g_prog_mu;
-std::deque<std::pair<std::string, std::shared_ptr<const Program>>> g_progs;   // newest last
+// Never destroyed (programs free device memory; at process exit the runtime may be gone).
+std::mutex& prog_mu() {
+    static auto* m = new std::mutex;
+    return *m;
+}
+std::deque<std::pair<std::string, std::shared_ptr<const Program>>>& progs() {   // newest last
+    static auto* d = new std::deque<std::pair<std::string, std::shared_ptr<const Program>>>;
+    return *d;
+}
 constexpr size_t kProgramCache = 16;
 
 std::string program_key(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc) {
@@ -635,29 +728,29 @@ std::shared_ptr<const Program> cached_program(const std::vector<GateDesc>& gates
         return std::make_shared<const Program>(compile(gates, n, fc, stream));
     const std::string key = program_key(gates, n, fc);
     {
-        std::lock_guard<std::mutex> lk(g_prog_mu);
-        for (auto it = g_progs.begin(); it != g_progs.end(); ++it) {
+        std::lock_guard<std::mutex> lk(prog_mu());
+        for (auto it = progs().begin(); it != progs().end(); ++it) {
             if (it->first == key) {
                 auto hit = *it;
-                g_progs.erase(it);
-                g_progs.push_back(hit);
+                progs().erase(it);
+                progs().push_back(hit);
                 return hit.second;
             }
         }
     }
     auto prog = std::make_shared<const Program>(compile(gates, n, fc, stream));
     cuda_check(cudaStreamSynchronize(stream), "program upload");   // usable from any stream
-    std::lock_guard<std::mutex> lk(g_prog_mu);
-    g_progs.emplace_back(key, prog);
-    if (g_progs.size() > kProgramCache) g_progs.pop_front();
+    std::lock_guard<std::mutex> lk(prog_mu());
+    progs().emplace_back(key, prog);
+    if (progs().size() > kProgramCache) progs().pop_front();
     return prog;
 }
 
 }  // namespace
 
 void clear_program_cache() {
-    std::lock_guard<std::mutex> lk(g_prog_mu);
-    g_progs.clear();
+    std::lock_guard<std::mutex> lk(prog_mu());
+    progs().clear();
 }
 
 void apply_circuit(lqcs_state& st, const std::vector<GateDesc>& gates, const FusionConfig& fc) {

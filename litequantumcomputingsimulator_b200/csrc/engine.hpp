@@ -101,6 +101,10 @@ void clear_autotune_cache();
 uint32_t default_fusion_width();
 // Drop the compiled programs kept for repeated circuits (apply_circuit).
 void clear_program_cache();
+// Free the amplitude buffers kept for new states of the same size.
+void clear_state_pool();
+// Called by ~lqcs_state: keeps a small amplitude buffer for the next state of its size.
+void pool_return(lqcs_state& st);
 
 // Compile a list of unitary gates to a Program (fused or gate by gate).
 Program compile(const std::vector<GateDesc>& gates, uint32_t n, const FusionConfig& fc,
@@ -135,6 +139,7 @@ struct lqcs_state {
     uint64_t len() const { return uint64_t{1} << n; }
     double* partials(size_t values);   // scratch for `values` reduced outputs
     void sync() const;
+    ~lqcs_state();   // hands a small amplitude buffer to the state pool
 };
 
 // A compiled circuit handle of the C ABI.
