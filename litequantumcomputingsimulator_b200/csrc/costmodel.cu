@@ -168,6 +168,7 @@ __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ t, 
 struct Model {
     std::vector<float> w;   // host copy of the trained parameters
     bool trained = false;
+    uint64_t version = 0;   // bumped whenever the weights change
 };
 std::mutex g_mu;
 Model g_model;
@@ -257,6 +258,7 @@ float costmodel_train(const float* features, const float* targets, uint64_t n, u
     std::lock_guard<std::mutex> lk(g_mu);
     g_model.w = std::move(w);
     g_model.trained = true;
+    ++g_model.version;
     return loss;
 }
 
@@ -315,6 +317,7 @@ void costmodel_set_weights(const float* w, uint64_t n) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_model.w.assign(w, w + n);
     g_model.trained = true;
+    ++g_model.version;
 }
 
 std::array<float, kCostFeatures> op_features(uint32_t kind, uint32_t width, uint32_t min_target,
@@ -358,6 +361,12 @@ void costmodel_clear() {
     std::lock_guard<std::mutex> lk(g_mu);
     g_model.w.clear();
     g_model.trained = false;
+    ++g_model.version;
+}
+
+uint64_t costmodel_version() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_model.version;
 }
 
 }  // namespace lqcs_b200

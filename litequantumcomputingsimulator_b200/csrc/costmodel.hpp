@@ -33,6 +33,7 @@ std::vector<float> costmodel_weights();
 void costmodel_set_weights(const float* w, uint64_t n);
 bool costmodel_trained();
 void costmodel_clear();
+uint64_t costmodel_version();   // changes whenever the weights change
 
 // Predicted device time (ms) of a list of device operations on n qubits.
 double predict_ops_ms(const std::vector<DevOp>& ops, uint32_t n);
