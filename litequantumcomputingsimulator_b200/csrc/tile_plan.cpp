@@ -37,6 +37,7 @@ TileConfig default_tile_config(uint32_t n) {
     c.L = static_cast<uint32_t>(env_int("LQCS_TILE_LOW", 5));
     c.inner = static_cast<uint32_t>(env_int("LQCS_TILE_INNER", 2));
     c.reg = env_int("LQCS_TILE_REG", 1) != 0;
+    c.search = env_int("LQCS_TILE_SEARCH", 1) != 0;
     c.m = std::max<uint32_t>(kTileMinBits, std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n));
     c.L = std::min<uint32_t>(std::min(c.L, c.m), kTileMinBits);   // column bits come from the thread index
     if (c.m - c.L > kTileMaxHigh) c.L = c.m - kTileMaxHigh;
@@ -55,6 +56,87 @@ static bool tile_requirements(const GateDesc& g, const TileConfig& c, std::vecto
     for (uint32_t j = 0; j < k; ++j) need.push_back(g.targets()[j]);
     (void)c;
     return true;
+}
+
+// First-fit picks the high tile qubits in the order gates ask for them, which is often not
+// the set that takes the most gates.  Local search: swap one high qubit of the pass for one
+// outside it while that lets the pass take more gates (same rules as the first-fit scan:
+// program order per qubit, barriers end the pass, at most kTileMaxOps gates).  On the
+// 30-qubit brickwork this cuts 75 passes to about 50.
+static void improve_high_bits(const std::vector<GateDesc>& gates, uint32_t n, const TileConfig& cfg,
+                              const std::vector<uint32_t>& remaining, std::vector<uint32_t>& hset,
+                              std::vector<uint32_t>& taken, std::vector<uint32_t>& deferred) {
+    struct G {
+        uint64_t qubits, need;   // all qubits; high qubits the gate needs in the tile
+        bool ok, barrier;
+    };
+    std::vector<G> gs;
+    gs.reserve(remaining.size());
+    std::vector<uint32_t> need;
+    for (uint32_t gi : remaining) {
+        const GateDesc& g = gates[gi];
+        G e{0, 0, false, g.type == LQCS_GATE_BARRIER};
+        for (uint32_t q : g.qubits) e.qubits |= uint64_t{1} << q;
+        if (!e.barrier && tile_requirements(g, cfg, need)) {
+            e.ok = true;
+            for (uint32_t q : need)
+                if (q >= cfg.L) e.need |= uint64_t{1} << q;
+        }
+        gs.push_back(e);
+    }
+    auto count = [&](uint64_t hmask) {
+        uint64_t blocked = 0;
+        size_t got = 0;
+        for (const G& e : gs) {
+            if (e.barrier || got >= kTileMaxOps) break;
+            if (!(e.qubits & blocked) && e.ok && !(e.need & ~hmask)) ++got;
+            else blocked |= e.qubits;
+        }
+        return got;
+    };
+    uint64_t hmask = 0;
+    for (uint32_t q : hset) hmask |= uint64_t{1} << q;
+    // with the padded set fixed the scan takes every gate first-fit took (and maybe more)
+    size_t best = count(hmask);
+    for (int round = 0; round < 8; ++round) {
+        bool better = false;
+        for (uint32_t out = cfg.L; out < n; ++out) {
+            if (!((hmask >> out) & 1)) continue;
+            for (uint32_t in = cfg.L; in < n; ++in) {
+                if ((hmask >> in) & 1) continue;
+                const uint64_t cand = (hmask & ~(uint64_t{1} << out)) | (uint64_t{1} << in);
+                const size_t c = count(cand);
+                if (c > best) {
+                    best = c;
+                    hmask = cand;
+                    better = true;
+                    break;
+                }
+            }
+        }
+        if (!better) break;
+    }
+    hset.clear();
+    for (uint32_t q = cfg.L; q < n; ++q)
+        if ((hmask >> q) & 1) hset.push_back(q);
+    taken.clear();
+    deferred.clear();
+    uint64_t blocked = 0;
+    bool stop = false;
+    for (size_t i = 0; i < gs.size(); ++i) {
+        const G& e = gs[i];
+        if (stop || e.barrier || taken.size() >= kTileMaxOps) {
+            stop = true;
+            deferred.push_back(remaining[i]);
+            continue;
+        }
+        if (!(e.qubits & blocked) && e.ok && !(e.need & ~hmask)) {
+            taken.push_back(remaining[i]);
+        } else {
+            deferred.push_back(remaining[i]);
+            blocked |= e.qubits;
+        }
+    }
 }
 
 std::vector<PlanItem> plan_tiles(const std::vector<GateDesc>& gates, uint32_t n,
@@ -120,6 +202,7 @@ std::vector<PlanItem> plan_tiles(const std::vector<GateDesc>& gates, uint32_t n,
         // every pass gets the full tile size: pad H with unused high qubits
         for (uint32_t q = cfg.L; q < n && hset.size() < h; ++q)
             if (std::find(hset.begin(), hset.end(), q) == hset.end()) hset.push_back(q);
+        if (cfg.search && n <= 64) improve_high_bits(gates, n, cfg, remaining, hset, taken, deferred);
         PlanItem it;
         it.is_pass = true;
         std::sort(hset.begin(), hset.end());

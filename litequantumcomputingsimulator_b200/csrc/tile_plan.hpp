@@ -13,6 +13,7 @@ struct TileConfig {
     uint32_t L = 5;        // low qubits always in the tile
     uint32_t inner = 2;    // widest dense operation fused inside a pass
     bool reg = true;       // register tile kernel where the pass fits it
+    bool search = true;    // local search over each pass's high qubits (LQCS_TILE_SEARCH=0: off)
 };
 TileConfig default_tile_config(uint32_t n);
 
