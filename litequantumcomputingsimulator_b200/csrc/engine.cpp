@@ -483,8 +483,9 @@ static Program compile_autotuned(const std::vector<GateDesc>& gates, uint32_t n,
 // Learned planning: every candidate plan (greedy dense blocks of width 1..6, tile passes of
 // several shapes) is scored by the cost model's predicted device time, and the best few
 // (two; LQCS_LEARNED_JUDGE sets how many, 1 = the model's choice alone) are then applied
-// once on a scratch state: measured wall time judges between the model's favourites, which
-// catches its ranking errors at a fraction of the autotuner's cost.  The choice is kept per
+// once on a scratch state with the default plan: measured wall time judges between the
+// model's favourites and the default, which catches the model's ranking errors at a
+// fraction of the autotuner's cost.  The choice is kept per
 // circuit and set of weights.  Without trained weights the plain greedy plan is used.
 static Program compile_learned(const std::vector<GateDesc>& gates, uint32_t n,
                                const FusionConfig& fc, cudaStream_t stream) {
@@ -526,6 +527,16 @@ static Program compile_learned(const std::vector<GateDesc>& gates, uint32_t n,
     if (judge >= 2 && scored.size() >= 2) {
         std::vector<TuneCandidate> shortlist;
         for (size_t i = 0; i < std::min(judge, scored.size()); ++i) shortlist.push_back(scored[i].second);
+        // and the default plan, so the judged choice is never slower than it
+        if (n >= kTileMinBits) {
+            TuneCandidate d;
+            d.cfg = default_tile_config(n);
+            bool have = false;
+            for (const TuneCandidate& c : shortlist)
+                have |= c.planner == 0 && c.cfg.m == d.cfg.m && c.cfg.L == d.cfg.L &&
+                        c.cfg.inner == d.cfg.inner;
+            if (!have) shortlist.push_back(d);
+        }
         const std::vector<double> ms = time_candidates(gates, n, shortlist);
         if (!ms.empty())
             pick = shortlist[std::min_element(ms.begin(), ms.end()) - ms.begin()];
