@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <tuple>
 
 #include "tile_plan.hpp"
 
@@ -916,6 +917,14 @@ RegLayout make_layout(uint32_t S, uint32_t W, uint32_t m) {
     return ly;
 }
 
+// Whether the tile bits in `lanes` cover all three residues mod 3 (see make_layout).
+bool residues_spread(uint32_t lanes) {
+    uint32_t seen = 0;
+    for (uint32_t b = 0; b < 32; ++b)
+        if ((lanes >> b) & 1) seen |= 1u << (b % 3);
+    return seen == 7u;
+}
+
 // `count` warp bits out of `avail`: the tile bits the pending dense operations target least
 // (ties: the higher bit), so that few later operations need a bit that is a warp bit.
 uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pending,
@@ -933,16 +942,31 @@ uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint3
         }
         if (best >= 0) W |= 1u << best;
     }
+    // lanes without a residue mod 3: trade a warp bit for a lane bit as little used
+    if (!residues_spread(avail & ~W)) {
+        for (uint32_t w = 0; w < 32; ++w) {
+            if (!((W >> w) & 1)) continue;
+            for (uint32_t l = 0; l < 32; ++l) {
+                const uint32_t W2 = (W & ~(1u << w)) | (1u << l);
+                if (((avail & ~W) >> l) & 1 && usage[l] <= usage[w] &&
+                    residues_spread(avail & ~W2))
+                    return W2;
+            }
+        }
+    }
     return W;
 }
 
 // Register sets of size kRegBits inside `allowed` that contain `must`, best first by
-// (ops applied now, dense ops covered later, usable as the final layout).
+// (ops applied now, dense ops covered later, usable as the final layout, and — when the
+// warp bits are known, `lane_pool` being the tile bits outside them — lanes that take all
+// three residues mod 3, which keeps the remaps free of bank conflicts).
 uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
-                    std::vector<uint32_t>& pending, uint32_t must, uint32_t allowed, uint32_t m) {
+                    std::vector<uint32_t>& pending, uint32_t must, uint32_t allowed, uint32_t m,
+                    uint32_t lane_pool = 0) {
     uint32_t best = 0;
     size_t best_now = 0, best_later = 0;
-    bool best_final = false, have = false;
+    bool best_final = false, best_spread = false, have = false;
     const uint32_t lanes = (1u << kLaneBits) - 1u;
     for (uint32_t S = 0; S < (1u << m); ++S) {
         if (__builtin_popcount(S) != static_cast<int>(kRegBits) || (S & must) != must ||
@@ -951,13 +975,15 @@ uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use
         const size_t now = scan(ops, use, pending, S, nullptr);
         const size_t later = covered(ops, pending, S);
         const bool fin = (S & lanes) == 0;
-        if (!have || now > best_now || (now == best_now && later > best_later) ||
-            (now == best_now && later == best_later && fin && !best_final)) {
+        const bool spread = lane_pool != 0 && residues_spread(lane_pool & ~S);
+        const auto key = std::make_tuple(now, later, fin, spread);
+        if (!have || key > std::make_tuple(best_now, best_later, best_final, best_spread)) {
             have = true;
             best = S;
             best_now = now;
             best_later = later;
             best_final = fin;
+            best_spread = spread;
         }
     }
     return best;
@@ -1102,7 +1128,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
         if (pending.empty()) break;
         const uint32_t must = target_mask(ops[pending.front()]);
         if ((must & W) == 0) {   // warp-local: the warp bits stay
-            S = choose_set(ops, use, pending, must, all & ~W, m);
+            S = choose_set(ops, use, pending, must, all & ~W, m, all & ~W);
             cur = layout_index(S, W);
             seq.emplace_back(-1, cur);
         } else {                 // a target is a warp bit: new warp bits, CTA-wide remap
