@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
     ap.add_argument("--extras", default=None,
                     help="comma-separated extra legs to run (sweep, unfused, qft, trajectories, "
-                         "width6, autotune, ragged, dm, costmodel, config0, kernels, adjoint); default all")
+                         "width6, autotune, ragged, dm, costmodel, config0, kernels, adjoint, shor); "
+                         "default all")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -228,9 +229,17 @@ def reference_arm(args):
 def cpu_side_baselines(ref) -> dict:
     """The reference's own CPU methods for the batched legs, on bounded samples (same run,
     all host cores): the parameter-shift gradient of one config-2 parameter set, and one
-    config-3 trajectory over the first 2 of its 20 layers (scaled by 10, stated)."""
+    config-3 trajectory over the first 2 of its 20 layers (scaled by 10, stated), and
+    algorithms::shor(119) with seed 9 (21 qubits, one period-finding round)."""
     from litequantumcomputingsimulator_b200 import workloads as W
     out = {}
+    try:
+        t0 = time.perf_counter()
+        r = ref.shor(119, 64, 10, 9)
+        out["shor_21q_s"] = time.perf_counter() - t0
+        out["shor_21q_factors"] = [r["factor1"], r["factor2"]]
+    except Exception as ex:  # noqa: BLE001
+        out["shor_error"] = str(ex)
     try:
         pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
         ham = W.random_hamiltonian(16, 500, seed=12)
@@ -733,6 +742,39 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["config0_min_margin"] = margin0
         except Exception as ex:  # noqa: BLE001
             out["config0_error"] = str(ex)
+
+    # Shor's period finding (a caller of the controlled-permutation kernel): one controlled
+    # modular multiplication y -> 2^(2^19) y mod 899 on the bench state (control qubit 19,
+    # work qubits 20..29), CUDA-event timed over 3 launches, GB/s from 32 B per amplitude of
+    # the control-1 half; then seeded algorithms.shor end to end at 21 qubits (N = 119, the
+    # reference's CPU sample) and at 30 qubits (N = 899 = 29 * 31: 20 counting + 10 work)
+    if want("shor") and n == 30:
+        try:
+            mx = lq.algorithms.modular_exponentiation(2, 899, 20, 10)
+            one = lq.QuantumCircuit(n)
+            one.append(mx.instructions()[19])
+            pk = lq.simulator.CompiledCircuit(one, fuse_gates=False)
+            pk.apply(sv)
+            torch.cuda.synchronize()
+            s.record()
+            for _ in range(3):
+                pk.apply(sv)
+            e.record()
+            torch.cuda.synchronize()
+            ms = s.elapsed_time(e) / 3
+            out["shor_modmul_ms"] = ms
+            out["shor_modmul_gbs"] = W.alg_bytes(one) / (ms / 1e3) / 1e9
+            lq.algorithms.shor(119, 64, 10, 9)   # warm-up: planning, allocations
+            for tag, N_, seed in (("21q", 119, 9), ("30q", 899, 1)):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r = lq.algorithms.shor(N_, 64, 10, seed)
+                dt = time.perf_counter() - t0
+                out[f"shor_{tag}"] = {"N": N_, "seed": seed, "s": dt, "success": r.success,
+                                      "factors": [r.factor1, r.factor2], "a": r.a,
+                                      "period": r.period, "attempts": r.attempts}
+        except Exception as ex:  # noqa: BLE001
+            out["shor_error"] = str(ex)
 
     # primitive kernels one gate (or reduction) at a time on the bench state, unfused: the
     # gate kernels (1q at the lowest and highest target, controlled, phase, 2q dense, 2q

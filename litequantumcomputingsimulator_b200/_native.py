@@ -166,6 +166,7 @@ SIGNATURES = {
     "lqcs_fusion_plan": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_int32, C.c_int32,
                                    C.c_uint64, C.c_void_p, C.c_void_p, _P(C.c_uint64)]),
     "lqcs_rng_uniforms": (C.c_int, [C.c_uint64, C.c_uint64, C.c_void_p]),
+    "lqcs_rng_u64": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p]),
     "lqcs_autotune": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, C.c_uint64,
                                 _P(TuneEntry), _P(C.c_uint64)]),
     "lqcs_dm_create": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64, _P(SimOptions),

@@ -534,6 +534,15 @@ int lqcs_rng_uniforms(uint64_t seed, uint64_t count, double* out) {
     });
 }
 
+int lqcs_rng_u64(uint64_t seed, uint64_t skip, uint64_t count, uint64_t* out) {
+    return guarded([&] {
+        if (count > 0) need(out, "out");
+        lqcs_b200::Rng rng(seed);
+        rng.discard(skip);
+        for (uint64_t i = 0; i < count; ++i) out[i] = rng();
+    });
+}
+
 int lqcs_fusion_plan(uint32_t n_qubits, const lqcs_instruction* insts, uint64_t n_insts,
                      int32_t max_fusion_width, int32_t fusion_mode, uint64_t cap,
                      uint32_t* block_width, uint32_t* block_gates, uint64_t* n_blocks) {

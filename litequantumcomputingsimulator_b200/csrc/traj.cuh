@@ -47,6 +47,13 @@ void launch_traj_tail_measure(const LaunchCtx& ctx, const double2* st, uint32_t 
                               uint32_t batch, uint32_t q, const BitList& fixed, uint64_t* vals,
                               uint32_t clbit, uint32_t uniform_index, const double* d_uniforms,
                               uint64_t first, uint64_t per_shot, TrajScratch& s);
+// Joint distribution of measured qubits mq[0..m-1] of one state: table[t] = sum of |a|^2
+// over the amplitudes whose bit mq[j] equals bit j of t, summed in a fixed order (chunks of
+// the free indices, then the chunks in order).  `partial` holds 2^m * chunks doubles, where
+// chunks = marginal_chunks(n, m).
+uint64_t marginal_chunks(uint32_t n, uint32_t m);
+void launch_marginal_table(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                           const uint32_t* mq, uint32_t m, double* partial, double* table);
 // Per-state choice into a table of normalised 2x2 operators (choice < 0: no-op).
 void launch_traj_table(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
                        const double2* d_mats, const int* d_choice);

@@ -260,7 +260,83 @@ __global__ void k_b_tail_decide(const double* __restrict__ partials, uint32_t nb
     regs[b] = outcome ? (regs[b] | bit) : (regs[b] & ~bit);
 }
 
+struct MarginalArgs {
+    uint8_t mq[kMaxQubits];   // measured qubit of table bit j
+    uint32_t m;
+    uint32_t log_chunks;
+    uint64_t free_mask;       // bits of the unmeasured qubits
+    uint64_t chunk;           // free indices per chunk
+};
+
+// Thread (t, c): table entry t, chunk c of the free indices (enumerated in increasing order
+// by the masked increment cur = ((cur | ~free) + 1) & free).  Consecutive threads take
+// consecutive t, so measured low qubits give coalesced reads.
+__global__ void __launch_bounds__(kThreads) k_marginal_partial(const double2* __restrict__ st,
+                                                               MarginalArgs a,
+                                                               double* __restrict__ partial) {
+    const uint64_t entries = uint64_t{1} << a.m;
+    const uint64_t gid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= (entries << a.log_chunks)) return;
+    const uint64_t t = gid & (entries - 1), c = gid >> a.m;
+    uint64_t base = 0;
+    for (uint32_t j = 0; j < a.m; ++j) base |= ((t >> j) & 1u) << a.mq[j];
+    // deposit of the chunk's first free index c * chunk into the free bit positions
+    uint64_t w = c * a.chunk, cur = 0, rest = a.free_mask;
+    while (w != 0 && rest != 0) {
+        const uint64_t low = rest & (~rest + 1);
+        if (w & 1u) cur |= low;
+        w >>= 1;
+        rest &= rest - 1;
+    }
+    double sum = 0.0;
+    for (uint64_t k = 0; k < a.chunk; ++k) {
+        const double2 v = __ldg(st + (base | cur));
+        sum += v.x * v.x + v.y * v.y;
+        cur = ((cur | ~a.free_mask) + 1) & a.free_mask;
+    }
+    partial[c * entries + t] = sum;
+}
+
+__global__ void k_marginal_sum(const double* __restrict__ partial, uint64_t entries,
+                               uint64_t chunks, double* __restrict__ table) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= entries) return;
+    double s = 0.0;
+    for (uint64_t c = 0; c < chunks; ++c) s += partial[c * entries + t];
+    table[t] = s;
+}
+
 }  // namespace
+
+uint64_t marginal_chunks(uint32_t n, uint32_t m) {
+    // about 2^21 threads in all, at most one chunk per free index
+    const uint32_t lc = m >= 21 ? 0u : std::min<uint32_t>(21u - m, n - m);
+    return uint64_t{1} << lc;
+}
+
+void launch_marginal_table(const LaunchCtx& ctx, const double2* st, uint32_t n,
+                           const uint32_t* mq, uint32_t m, double* partial, double* table) {
+    MarginalArgs a{};
+    uint64_t meas = 0;
+    for (uint32_t j = 0; j < m; ++j) {
+        a.mq[j] = static_cast<uint8_t>(mq[j]);
+        meas |= uint64_t{1} << mq[j];
+    }
+    a.m = m;
+    const uint64_t chunks = marginal_chunks(n, m);
+    a.log_chunks = static_cast<uint32_t>(__builtin_ctzll(chunks));
+    a.free_mask = ((uint64_t{1} << n) - 1) & ~meas;
+    a.chunk = (uint64_t{1} << (n - m)) >> a.log_chunks;
+    const uint64_t entries = uint64_t{1} << m, threads = entries * chunks;
+    k_marginal_partial<<<static_cast<unsigned>((threads + kThreads - 1) / kThreads), kThreads, 0,
+                         ctx.stream>>>(st, a, chunks == 1 ? table : partial);
+    check_launch("marginal_partial");
+    if (chunks > 1) {
+        k_marginal_sum<<<static_cast<unsigned>((entries + 255) / 256), 256, 0, ctx.stream>>>(
+            partial, entries, chunks, table);
+        check_launch("marginal_sum");
+    }
+}
 
 void launch_traj_kraus(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch, uint32_t q,
                        const TrajDecide& d, const double* d_uniforms, uint64_t first,

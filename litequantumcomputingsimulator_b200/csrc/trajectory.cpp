@@ -337,6 +337,125 @@ void run_fused(const FusedRun& f, uint64_t* regs) {
     for (uint64_t p = 0; p < f.shots; ++p) regs[order[p]] = regs_perm[p];
 }
 
+uint64_t stretch_qubits(const std::vector<GateDesc>& s) {
+    uint64_t m = 0;
+    for (const GateDesc& g : s)
+        for (uint32_t q : g.qubits) m |= uint64_t{1} << q;
+    return m;
+}
+
+// Shared deterministic prefix.  When nothing before the final measurements is random (no
+// noise model, no Kraus instruction, no Reset, no earlier Measure), every shot reaches them
+// in the same state.  Unitaries between those measurements are moved ahead of them when
+// they touch no qubit measured before them (a unitary and a projective measurement on
+// disjoint qubits commute) and dropped when no measurement follows them (they cannot change
+// a recorded outcome); the reference's one-qubit fusion leaves such gates there, because a
+// Measure flushes only its own qubit's pending product (src/transpiler/gate_fusion.cpp:
+// 58-62), and they send the reference down its per-shot path.  One state is evolved, the
+// joint distribution of the measured qubits is tabulated once, and each shot walks its
+// measurements with its own uniforms: outcome 1 iff u < P(bit = 1 | earlier outcomes) —
+// the Born rule on the subspace consistent with the earlier outcomes, as the terminal
+// measurements of the batched path decide.  Returns false (nothing done) when the circuit
+// does not have this form or the table would exceed 2^24 entries.
+bool run_shared_prefix(uint32_t n, const std::vector<Item>& items,
+                       const std::vector<std::vector<GateDesc>>& stretches, const FusionConfig& fc,
+                       const std::vector<double>& u, uint32_t K, uint64_t shots, uint64_t* regs) {
+    // tail: the longest suffix of Measures (distinct qubits) and unitaries
+    size_t b = items.size();
+    {
+        uint64_t seen = 0;
+        while (b > 0) {
+            const Item& it = items[b - 1];
+            if (it.kind == kMeasure) {
+                if ((seen >> it.q) & 1) break;
+                seen |= uint64_t{1} << it.q;
+            } else if (it.kind != kUnitary) {
+                break;
+            }
+            --b;
+        }
+    }
+    // shrink until every unitary of the tail commutes with the measurements before it
+    std::vector<size_t> hoist;
+    while (true) {
+        hoist.clear();
+        uint64_t measured = 0;
+        size_t bad = items.size();
+        for (size_t i = b; i < items.size(); ++i) {
+            const Item& it = items[i];
+            if (it.kind == kMeasure) {
+                measured |= uint64_t{1} << it.q;
+                continue;
+            }
+            bool later = false;
+            for (size_t j = i + 1; j < items.size(); ++j) later |= items[j].kind == kMeasure;
+            if (!later) continue;   // dropped
+            if ((stretch_qubits(stretches[it.prog]) & measured) == 0) {
+                hoist.push_back(i);
+                continue;
+            }
+            bad = i;
+            break;
+        }
+        if (bad == items.size()) break;
+        b = bad + 1;
+    }
+    for (size_t i = 0; i < b; ++i)
+        if (items[i].kind != kUnitary) return false;
+    std::vector<uint32_t> mq, clb, uid;
+    for (size_t i = b; i < items.size(); ++i)
+        if (items[i].kind == kMeasure) {
+            mq.push_back(items[i].q);
+            clb.push_back(items[i].clbit);
+            uid.push_back(items[i].uidx);
+        }
+    const uint32_t m = static_cast<uint32_t>(mq.size());
+    if (m == 0 || m > 24) return false;
+
+    std::vector<GateDesc> prefix;
+    for (size_t i = 0; i < b; ++i)
+        prefix.insert(prefix.end(), stretches[items[i].prog].begin(), stretches[items[i].prog].end());
+    for (size_t i : hoist)
+        prefix.insert(prefix.end(), stretches[items[i].prog].begin(), stretches[items[i].prog].end());
+
+    auto st = new_state(n, 1, nullptr);
+    const LaunchCtx ctx = st->ctx;
+    launch_set_basis(ctx, st->d(), n, 1, 0);
+    Program prog;
+    if (!prefix.empty()) {
+        prog = compile(prefix, n, fc, nullptr);
+        prog.launch(ctx, st->d(), n, 1);
+    }
+    const uint64_t entries = uint64_t{1} << m;
+    DeviceBuffer partial, table;
+    partial.ensure(sizeof(double) * entries * marginal_chunks(n, m));
+    table.ensure(sizeof(double) * entries);
+    launch_marginal_table(ctx, st->d(), n, mq.data(), m, partial.as<double>(), table.as<double>());
+    // level sums: lev[j][o] = total over the entries whose low j bits equal o
+    std::vector<std::vector<double>> lev(m + 1);
+    lev[m].resize(entries);
+    cuda_check(cudaMemcpyAsync(lev[m].data(), table.ptr, sizeof(double) * entries,
+                               cudaMemcpyDeviceToHost, ctx.stream), "D2H marginal table");
+    cuda_check(cudaStreamSynchronize(ctx.stream), "marginal table");
+    for (uint32_t j = m; j-- > 0;) {
+        lev[j].resize(uint64_t{1} << j);
+        for (uint64_t o = 0; o < (uint64_t{1} << j); ++o)
+            lev[j][o] = lev[j + 1][o] + lev[j + 1][o | (uint64_t{1} << j)];
+    }
+    for (uint64_t s = 0; s < shots; ++s) {
+        uint64_t o = 0, reg = 0;
+        for (uint32_t j = 0; j < m; ++j) {
+            const double r0 = lev[j + 1][o], r1 = lev[j + 1][o | (uint64_t{1} << j)];
+            const int outcome = u[s * K + uid[j]] < r1 / (r0 + r1) ? 1 : 0;
+            o |= static_cast<uint64_t>(outcome) << j;
+            const uint64_t bit = uint64_t{1} << clb[j];
+            reg = outcome ? (reg | bit) : (reg & ~bit);
+        }
+        regs[s] = reg;
+    }
+    return true;
+}
+
 }  // namespace
 
 void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64_t shots,
@@ -457,6 +576,8 @@ void run_per_shot_batched(uint32_t n, const std::vector<GateDesc>& gates, uint64
                    "H2D branch table");
         choice_host[i] = std::move(ch);
     }
+
+    if (!noisy && run_shared_prefix(n, items, stretches, fc, u, K, shots, regs)) return;
 
     if (fc_in.fuse && use_fused(n)) {
         std::vector<std::vector<Kraus>> norm(channels.size());

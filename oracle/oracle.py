@@ -547,6 +547,8 @@ class Ref:
                 "lqcsref_dm_probabilities": (i, [u32, vp, u64, u64, vp, vp]),
                 "lqcsref_trajectories": (i, [u32, u32, vp, u64, u64, u64, u64, vp, vp]),
                 "lqcsref_uniforms": (None, [u64, u64, vp]),
+                "lqcsref_modexp_statevector": (i, [u64, u64, u32, u32, vp]),
+                "lqcsref_shor": (i, [u64, u64, u64, i, u64, vp, vp, vp, u64, vp]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(lib, name)
@@ -681,3 +683,25 @@ class Ref:
         out = np.empty(count)
         self.lib.lqcsref_uniforms(seed, count, out.ctypes.data)
         return out
+
+    def modexp_statevector(self, a: int, N: int, n_count: int, n_work: int) -> np.ndarray:
+        """run_statevector of X(work 0), H on the counting qubits and
+        algorithms::modular_exponentiation(a, N, n_count, n_work)."""
+        out = np.empty(1 << (n_count + n_work), dtype=np.complex128)
+        self._check(self.lib.lqcsref_modexp_statevector(a, N, n_count, n_work, out.ctypes.data))
+        return out
+
+    def shor(self, N: int, shots: int = 64, max_attempts: int = 10,
+             seed: Optional[int] = None) -> dict:
+        """algorithms::shor: {success, factor1, factor2, a, period, attempts, counts}."""
+        info = np.zeros(6, dtype=np.uint64)
+        keys = np.zeros(max(shots, 1), dtype=np.uint64)
+        counts = np.zeros_like(keys)
+        nout = C.c_uint64(0)
+        self._check(self.lib.lqcsref_shor(N, shots, max_attempts, 0 if seed is None else 1,
+                                          0 if seed is None else seed, info.ctypes.data,
+                                          keys.ctypes.data, counts.ctypes.data, keys.size,
+                                          C.byref(nout)))
+        return {"success": bool(info[0]), "factor1": int(info[1]), "factor2": int(info[2]),
+                "a": int(info[3]), "period": int(info[4]), "attempts": int(info[5]),
+                "counts": {int(k): int(c) for k, c in zip(keys[: nout.value], counts[: nout.value])}}

@@ -451,6 +451,44 @@ int lqcsref_trajectories(uint32_t n, uint32_t nclbits, const lqcs_instruction* i
     });
 }
 
+// Period-finding register of algorithms::modular_exponentiation
+// (src/algorithms/arithmetic.cpp): work register |1>, H on every counting qubit, then the
+// controlled modular multiplications; the amplitudes of run_statevector.
+int lqcsref_modexp_statevector(uint64_t a, uint64_t N, uint32_t n_count, uint32_t n_work,
+                               double* out) {
+    return guarded([&] {
+        QuantumCircuit qc(n_count + n_work);
+        qc.x(static_cast<qubit_t>(n_count));
+        for (uint32_t j = 0; j < n_count; ++j) qc.h(static_cast<qubit_t>(j));
+        qc.compose(algorithms::modular_exponentiation(a, N, n_count, n_work));
+        StatevectorSimulator sim;
+        const Statevector sv = sim.run_statevector(qc);
+        std::memcpy(out, sv.data(), sizeof(complex_t) * sv.size());
+    });
+}
+
+// algorithms::shor (src/algorithms/shor.cpp): info = {success, factor1, factor2, a, period,
+// attempts}; the counts of the successful round as (register, count).
+int lqcsref_shor(uint64_t N, uint64_t shots, uint64_t max_attempts, int has_seed, uint64_t seed,
+                 uint64_t* info, uint64_t* keys, uint64_t* counts, uint64_t cap,
+                 uint64_t* n_out) {
+    return guarded([&] {
+        algorithms::ShorOptions o;
+        o.shots = shots;
+        o.max_attempts = max_attempts;
+        if (has_seed) o.seed = seed;
+        const algorithms::ShorResult r = algorithms::shor(N, o);
+        info[0] = r.success ? 1 : 0;
+        info[1] = r.factor1;
+        info[2] = r.factor2;
+        info[3] = r.a;
+        info[4] = r.period;
+        info[5] = r.attempts;
+        Result res(r.counts, shots);
+        write_counts(res, keys, counts, cap, n_out);
+    });
+}
+
 // Draw `count` uniforms from lqcs::Rng(seed) (include/lqcs/core/random.hpp).
 void lqcsref_uniforms(uint64_t seed, uint64_t count, double* out) {
     Rng rng(seed);

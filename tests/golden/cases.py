@@ -70,6 +70,24 @@ UNIFORMS = {
 }
 
 
+# algorithms::modular_exponentiation after X(work 0) and H on the counting register
+MODEXP = {
+    "modexp_7_15": {"a": 7, "N": 15, "n_count": 6, "n_work": 4},
+    "modexp_5_33": {"a": 5, "N": 33, "n_count": 5, "n_work": 6},
+}
+
+# algorithms::shor with a fixed seed (quantum rounds, lucky gcds, classical shortcuts)
+SHOR = {
+    "shor_15": {"N": 15, "shots": 64, "max_attempts": 10, "seed": 7},
+    "shor_35": {"N": 35, "shots": 64, "max_attempts": 10, "seed": 7},
+    "shor_55": {"N": 55, "shots": 64, "max_attempts": 10, "seed": 7},
+    "shor_91": {"N": 91, "shots": 128, "max_attempts": 10, "seed": 3},
+    "shor_21_gcd": {"N": 21, "shots": 64, "max_attempts": 10, "seed": 7},
+    "shor_27_power": {"N": 27, "shots": 64, "max_attempts": 10, "seed": 1},
+    "shor_97_prime": {"N": 97, "shots": 64, "max_attempts": 10, "seed": 1},
+}
+
+
 def circuit(spec: dict) -> lq.QuantumCircuit:
     gen, args, kwargs = spec["gen"], spec["args"], dict(spec.get("kwargs", {}))
     if gen == "random_circuit":

@@ -11,8 +11,9 @@ to the reference's own results on machines without it:
   (`DensityMatrixSimulator`), parameter-shift gradients (`algorithms::parameter_shift_gradient`),
   `Rng` uniforms;
 * reference_cases.json — the case descriptions (generator and arguments), the counts maps of
-  `StatevectorSimulator::run` (noiseless sampling, a noise model, explicit Kraus placements)
-  and the expectation values (`algorithms::expectation`).
+  `StatevectorSimulator::run` (noiseless sampling, a noise model, explicit Kraus placements),
+  the expectation values (`algorithms::expectation`) and seeded `algorithms::shor` results;
+* the period-finding register after `algorithms::modular_exponentiation` (amplitudes).
 
 Every circuit comes from the seeded generators of `litequantumcomputingsimulator_b200.workloads`
 and `tests/helpers.py`; changing either means running this script again:
@@ -77,6 +78,14 @@ def main() -> None:
     for name, spec in cases.UNIFORMS.items():
         arrays[name] = ref.uniforms(spec["seed"], spec["count"])
         meta[name] = spec
+    for name, spec in cases.MODEXP.items():
+        arrays[name] = ref.modexp_statevector(spec["a"], spec["N"], spec["n_count"],
+                                              spec["n_work"])
+        meta[name] = spec
+    for name, spec in cases.SHOR.items():
+        out = ref.shor(spec["N"], spec["shots"], spec["max_attempts"], spec["seed"])
+        out["counts"] = {str(k): v for k, v in sorted(out["counts"].items())}
+        meta[name] = dict(spec, result=out)
     np.savez_compressed(HERE / "reference_vectors.npz", **arrays)
     (HERE / "reference_cases.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     print(f"wrote {len(arrays)} arrays and {len(meta)} cases")

@@ -78,3 +78,93 @@ def test_oracle_uniforms_bit_exact(name):
     spec = G.UNIFORMS[name]
     g = MT64(spec["seed"])
     assert np.array_equal(g.uniforms(spec["count"]), ARRAYS[name])
+
+
+# ---- Shor's classical side (no GPU: these cases end before any period finding)
+
+@pytest.mark.parametrize("name", ["shor_21_gcd", "shor_27_power", "shor_97_prime"])
+def test_shor_classical_paths(name):
+    from litequantumcomputingsimulator_b200 import algorithms as A
+    spec = G.SHOR[name]
+    want = CASES[name]["result"]
+    got = A.shor(spec["N"], spec["shots"], spec["max_attempts"], spec["seed"])
+    for key in ("success", "factor1", "factor2", "a", "period", "attempts"):
+        assert getattr(got, key) == want[key], key
+    assert got.counts == {} and got.circuit is None
+
+
+@pytest.mark.parametrize("name", sorted(G.SHOR))
+def test_shor_first_base_draw(name):
+    """The first base equals the reference's std::uniform_int_distribution draw."""
+    from litequantumcomputingsimulator_b200 import algorithms as A
+    spec = G.SHOR[name]
+    want = CASES[name]["result"]
+    if want["attempts"] == 0:
+        pytest.skip("classical shortcut: no base drawn")
+    assert want["attempts"] == 1
+    assert A._Mt64Stream(spec["seed"]).uniform_int(2, spec["N"] - 2) == want["a"]
+
+
+def test_rng_u64_matches_uniforms():
+    """lqcs_rng_u64 gives the raw mt19937_64 draws (equal to the oracle's restatement, which
+    is pinned to the C++ standard's 10000th value), from any starting position."""
+    from litequantumcomputingsimulator_b200 import _native as N
+    for name in sorted(G.UNIFORMS):
+        spec = G.UNIFORMS[name]
+        raw = np.empty(spec["count"], dtype=np.uint64)
+        N.call("lqcs_rng_u64", spec["seed"], 0, raw.size, raw.ctypes.data)
+        g = MT64(spec["seed"])
+        assert [g.next_u64() for _ in range(raw.size)] == [int(v) for v in raw]
+        tail = np.empty(5, dtype=np.uint64)
+        N.call("lqcs_rng_u64", spec["seed"], 7, 5, tail.ctypes.data)
+        assert np.array_equal(tail, raw[7:12])
+
+
+def test_number_theory():
+    from fractions import Fraction
+    from litequantumcomputingsimulator_b200 import algorithms as A
+    primes = [n for n in range(2, 400) if all(n % d for d in range(2, int(n ** 0.5) + 1))]
+    assert [n for n in range(400) if A.is_prime(n)] == primes
+    for n in range(4, 5000):
+        b = A.perfect_power_base(n)
+        ks = [(r, k) for k in range(2, n.bit_length() + 1)
+              for r in (round(n ** (1 / k)) - 1, round(n ** (1 / k)), round(n ** (1 / k)) + 1)
+              if r >= 2 and r ** k == n]
+        assert b == (min(ks, key=lambda t: t[1])[0] if ks else 0), n
+    rng = np.random.default_rng(5)
+    for _ in range(300):
+        den = 1 << int(rng.integers(4, 24))
+        num = int(rng.integers(1, den))
+        lim = int(rng.integers(2, 2000))
+        got = A.continued_fraction_denominators(num, den, lim)
+        x, want, conv = Fraction(num, den), [], []
+        q2, q1, f = 1, 0, x
+        while True:   # convergent denominators by the textbook recurrence
+            a = f.numerator // f.denominator
+            q = a * q1 + q2
+            if q > lim:
+                break
+            want.append(q)
+            q2, q1 = q1, q
+            if f == a:
+                break
+            f = 1 / (f - a)
+        assert got == want
+
+
+def test_modular_exponentiation_builder():
+    from litequantumcomputingsimulator_b200 import algorithms as A
+    from litequantumcomputingsimulator_b200.circuit import GateType
+    qc = A.modular_exponentiation(7, 15, 3, 4)
+    insts = qc.instructions()
+    assert qc.num_qubits() == 7 and len(insts) == 3
+    for j, inst in enumerate(insts):
+        assert inst.gate.type == GateType.Permutation and inst.gate.n_controls == 1
+        assert list(inst.qubits) == [j, 3, 4, 5, 6]
+        f = pow(7, 1 << j, 15)
+        assert list(inst.gate.perm) == [(f * y) % 15 if y < 15 else y for y in range(16)]
+    for args in ((7, 1, 3, 4), (7, 33, 3, 4), (6, 15, 3, 4)):
+        with pytest.raises(ValueError):
+            A.modular_exponentiation(*args)
+    with pytest.raises(ValueError):
+        A.shor(3)

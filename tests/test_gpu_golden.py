@@ -79,3 +79,33 @@ def test_density_probabilities(name):
     sim = lq.DensityMatrixSimulator(noise=G.noise_model(spec.get("noise_model")))
     got = sim.run_density_matrix(qc).probabilities()
     assert np.max(np.abs(got - ARRAYS[name])) < TOL
+
+
+@pytest.mark.parametrize("name", sorted(G.MODEXP))
+@pytest.mark.parametrize("mode", [0, 3])
+def test_modular_exponentiation(name, mode):
+    """Controlled modular multiplications (singly controlled permutations of the work
+    register) after X(work 0) and H on the counting register."""
+    spec = G.MODEXP[name]
+    nc, nw = spec["n_count"], spec["n_work"]
+    qc = lq.QuantumCircuit(nc + nw)
+    qc.x(nc)
+    for j in range(nc):
+        qc.h(j)
+    qc.compose(lq.algorithms.modular_exponentiation(spec["a"], spec["N"], nc, nw))
+    got = lq.StatevectorSimulator(fusion_mode=mode).run_statevector(qc).to_numpy()
+    assert np.max(np.abs(got - ARRAYS[name])) < TOL
+
+
+@pytest.mark.parametrize("name", sorted(G.SHOR))
+def test_shor(name):
+    """Seeded Shor runs: base, period, factors, attempts and the successful round's counts
+    all equal the reference's."""
+    spec = G.SHOR[name]
+    want = CASES[name]["result"]
+    got = lq.algorithms.shor(spec["N"], spec["shots"], spec["max_attempts"], spec["seed"])
+    for key in ("success", "factor1", "factor2", "a", "period", "attempts"):
+        assert getattr(got, key) == want[key], key
+    n = 2 * spec["N"].bit_length()
+    keys = {format(int(k), "b").zfill(n): v for k, v in want["counts"].items()}
+    assert got.counts == keys

@@ -252,6 +252,30 @@ def test_collapse_reset_kraus(port, n):
                 assert abs(got - want) < TOL
 
 
+@pytest.mark.parametrize("a,N,nc,nw", [(2, 209, 8, 8), (7, 187, 6, 8), (5, 21, 14, 5)])
+def test_modular_exponentiation_vs_reference(ref, a, N, nc, nw):
+    """algorithms::modular_exponentiation on the tile path (>= 12 qubits): singly controlled
+    permutations of 5-8 work qubits between tile passes."""
+    want = ref.modexp_statevector(a, N, nc, nw)
+    qc = lq.QuantumCircuit(nc + nw)
+    qc.x(nc)
+    for j in range(nc):
+        qc.h(j)
+    qc.compose(lq.algorithms.modular_exponentiation(a, N, nc, nw))
+    got = lq.StatevectorSimulator().run_statevector(qc).to_numpy()
+    assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("N,seed", [(39, 2), (51, 5), (65, 11), (119, 9), (143, 6)])
+def test_shor_vs_reference(ref, N, seed):
+    want = ref.shor(N, 64, 10, seed)
+    got = lq.algorithms.shor(N, 64, 10, seed)
+    for key in ("success", "factor1", "factor2", "a", "period", "attempts"):
+        assert getattr(got, key) == want[key], key
+    n = 2 * N.bit_length()
+    assert got.counts == {format(k, "b").zfill(n): v for k, v in want["counts"].items()}
+
+
 def test_parameter_shift_matches_reference(ref):
     pc, theta = W.random_pauli_ansatz(6, 20, seed=5)
     h = W.random_hamiltonian(6, 30, seed=6)

@@ -151,3 +151,29 @@ def test_shot_ranges_concatenate_to_one_run(n):
     full = dm.run_registers(small, 80)
     parts = np.concatenate([dm.run_registers(small, 30), dm.run_registers(small, 50, shot_offset=30)])
     assert np.array_equal(full, parts)
+
+
+@pytest.mark.parametrize("n", [6, 13])
+def test_noiseless_per_shot_shares_one_state(ref, n):
+    """Noiseless circuits that the reference runs per shot because its one-qubit fusion
+    leaves gates between the final measurements (a Measure flushes only its own qubit):
+    one state, one table of the measured qubits, per-shot walks — counts identical to the
+    reference's, with measurements in any order and any clbit mapping, gates on unmeasured
+    qubits after the measurements, and a unitary that has to stay between them."""
+    rng = np.random.default_rng(n)
+    for trial in range(4):
+        qc = lq.QuantumCircuit(n, n)
+        qc.compose(W.brickwork(n, 3, seed=50 + trial))
+        for q in range(n):
+            qc.u(*(float(x) for x in rng.uniform(0, 6.3, 3)), q)
+        order = [int(x) for x in rng.permutation(n)]
+        clbits = [int(x) for x in rng.permutation(n)]
+        measured = order[: n - 2]
+        for k, q in enumerate(measured):
+            qc.measure(q, clbits[k])
+            if trial == 3 and k == 1:
+                qc.cx(measured[0], measured[2])   # touches a measured qubit: stays per-shot
+        qc.h(order[-1])                           # after every measurement: no effect
+        want = ref.run(qc, 500, 100 + trial)
+        got = counts_of(lq.StatevectorSimulator(seed=100 + trial).run_registers(qc, 500))
+        assert got == want
