@@ -405,25 +405,40 @@ __device__ __forceinline__ uint64_t local_offset(uint32_t l, const PPerm& p) {
     return o;
 }
 
+// Each block converts the cycle table to state offsets once (shared memory); a thread then
+// rotates every cycle of its group, eight elements per step: the eight source amplitudes of
+// a step are all still unwritten when they are loaded together (a step writes positions
+// i..i-7 and reads i-1..i-8), so eight loads are in flight instead of one.
+// Off: uint32_t when every target is below bit 32, else uint64_t.
+template <typename Off>
 __global__ void __launch_bounds__(kThreads) k_perm(double2* __restrict__ st, PPerm p) {
-    extern __shared__ uint32_t sm_cyc[];
-    uint32_t* s_len = sm_cyc + p.total_len;
-    for (uint32_t i = threadIdx.x; i < p.total_len; i += blockDim.x) sm_cyc[i] = p.cycles[i];
+    extern __shared__ __align__(8) unsigned char sm_raw[];
+    Off* sm_off = reinterpret_cast<Off*>(sm_raw);
+    uint32_t* s_len = reinterpret_cast<uint32_t*>(sm_off + p.total_len);
+    for (uint32_t i = threadIdx.x; i < p.total_len; i += blockDim.x)
+        sm_off[i] = static_cast<Off>(local_offset(p.cycles[i], p));
     for (uint32_t i = threadIdx.x; i < p.n_cycles; i += blockDim.x) s_len[i] = p.cycle_len[i];
     __syncthreads();
     double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
          g < p.n_groups; g += stride) {
-        const uint64_t base = expand_bits(g, p.fixed) | p.cmask;
+        double2* __restrict__ sg = s + (expand_bits(g, p.fixed) | p.cmask);
         uint32_t start = 0;
         for (uint32_t c = 0; c < p.n_cycles; ++c) {
             const uint32_t len = s_len[c];
-            const uint32_t* cyc = sm_cyc + start;
-            const double2 last = s[base | local_offset(cyc[len - 1], p)];
-            for (uint32_t i = len - 1; i > 0; --i)
-                s[base | local_offset(cyc[i], p)] = s[base | local_offset(cyc[i - 1], p)];
-            s[base | local_offset(cyc[0], p)] = last;
+            const Off* off = sm_off + start;
+            const double2 last = sg[off[len - 1]];
+            uint32_t i = len - 1;
+            for (; i >= 8; i -= 8) {
+                double2 t[8];
+#pragma unroll
+                for (uint32_t u = 0; u < 8; ++u) t[u] = sg[off[i - 1 - u]];
+#pragma unroll
+                for (uint32_t u = 0; u < 8; ++u) sg[off[i - u]] = t[u];
+            }
+            for (; i > 0; --i) sg[off[i]] = sg[off[i - 1]];
+            sg[off[0]] = last;
             start += len;
         }
     }
@@ -449,13 +464,23 @@ void launch_perm(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
     p.cycle_len = d_cycle_len;
     p.n_cycles = n_cycles;
     p.total_len = total_len;
-    const size_t smem = sizeof(uint32_t) * (total_len + n_cycles);
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_perm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-    }
+    uint32_t top = 0;
+    for (uint32_t j = 0; j < k; ++j) top = std::max(top, targets[j]);
+    const bool narrow = top < 32;
+    const size_t smem = (narrow ? sizeof(uint32_t) : sizeof(uint64_t)) * total_len +
+                        sizeof(uint32_t) * n_cycles;
     dim3 grid(grid_for(ctx, p.n_groups), batch);
-    k_perm<<<grid, kThreads, smem, ctx.stream>>>(st, p);
+    if (narrow) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_perm<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        k_perm<uint32_t><<<grid, kThreads, smem, ctx.stream>>>(st, p);
+    } else {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_perm<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        k_perm<uint64_t><<<grid, kThreads, smem, ctx.stream>>>(st, p);
+    }
     check_launch("perm");
 }
 
