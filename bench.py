@@ -744,15 +744,16 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["config0_error"] = str(ex)
 
     # Shor's period finding (a caller of the controlled-permutation kernel): one controlled
-    # modular multiplication y -> 2^(2^19) y mod 899 on the bench state (control qubit 19,
-    # work qubits 20..29), CUDA-event timed over 3 launches, GB/s from 32 B per amplitude of
-    # the control-1 half; then seeded algorithms.shor end to end at 21 qubits (N = 119, the
-    # reference's CPU sample) and at 30 qubits (N = 899 = 29 * 31: 20 counting + 10 work)
-    if want("shor") and n == 30:
+    # modular multiplication y -> 2^(2^(n-11)) y mod 899 on the bench state (control qubit
+    # n-11, work qubits n-10..n-1), CUDA-event timed over 3 launches, GB/s from 32 B per
+    # amplitude of the control-1 half; then seeded algorithms.shor end to end at 21 qubits
+    # (N = 119, the reference's CPU sample) and, on the 30-qubit bench, at 30 qubits
+    # (N = 899 = 29 * 31: 20 counting + 10 work)
+    if want("shor") and n >= 11:
         try:
-            mx = lq.algorithms.modular_exponentiation(2, 899, 20, 10)
+            mx = lq.algorithms.modular_exponentiation(2, 899, n - 10, 10)
             one = lq.QuantumCircuit(n)
-            one.append(mx.instructions()[19])
+            one.append(mx.instructions()[n - 11])
             pk = lq.simulator.CompiledCircuit(one, fuse_gates=False)
             pk.apply(sv)
             torch.cuda.synchronize()
@@ -765,7 +766,7 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["shor_modmul_ms"] = ms
             out["shor_modmul_gbs"] = W.alg_bytes(one) / (ms / 1e3) / 1e9
             lq.algorithms.shor(119, 64, 10, 9)   # warm-up: planning, allocations
-            for tag, N_, seed in (("21q", 119, 9), ("30q", 899, 1)):
+            for tag, N_, seed in (("21q", 119, 9), ("30q", 899, 1))[: 2 if n == 30 else 1]:
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 r = lq.algorithms.shor(N_, 64, 10, seed)
