@@ -243,10 +243,14 @@ def autotune(circuit) -> list:
 def registers_to_counts(regs: np.ndarray, n_clbits: int) -> dict:
     """Count per-shot classical registers as the reference's MSB-left key strings."""
     vals, cnt = np.unique(regs, return_counts=True)
-    out = {}
-    for v, c in zip(vals.tolist(), cnt.tolist()):
-        out[format(v, "b").zfill(n_clbits)[-n_clbits:] if n_clbits else ""] = int(c)
-    return out
+    if n_clbits == 0:
+        return {"": int(cnt.sum())} if vals.size else {}
+    # all keys at once: the bits as ASCII digits, MSB first, cut into n_clbits-wide strings
+    shifts = np.arange(n_clbits - 1, -1, -1, dtype=np.uint64)
+    digits = ((vals.astype(np.uint64)[:, None] >> shifts) & np.uint64(1)).astype(np.uint8) + 48
+    text = digits.tobytes().decode()
+    keys = [text[i:i + n_clbits] for i in range(0, len(text), n_clbits)]
+    return dict(zip(keys, cnt.tolist()))
 
 
 class StatevectorSimulator:
