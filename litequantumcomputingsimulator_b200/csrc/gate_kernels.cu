@@ -409,16 +409,19 @@ __device__ __forceinline__ uint64_t local_offset(uint32_t l, const PPerm& p) {
 // rotates every cycle of its group, eight elements per step: the eight source amplitudes of
 // a step are all still unwritten when they are loaded together (a step writes positions
 // i..i-7 and reads i-1..i-8), so eight loads are in flight instead of one.
-// Off: uint32_t when every target is below bit 32, else uint64_t.
-template <typename Off>
+// Off: uint32_t when every target is below bit 32, else uint64_t.  kShared = false (tables
+// too large for shared memory, 2^15 entries and up): offsets computed from the global table.
+template <typename Off, bool kShared>
 __global__ void __launch_bounds__(kThreads) k_perm(double2* __restrict__ st, PPerm p) {
     extern __shared__ __align__(8) unsigned char sm_raw[];
     Off* sm_off = reinterpret_cast<Off*>(sm_raw);
     uint32_t* s_len = reinterpret_cast<uint32_t*>(sm_off + p.total_len);
-    for (uint32_t i = threadIdx.x; i < p.total_len; i += blockDim.x)
-        sm_off[i] = static_cast<Off>(local_offset(p.cycles[i], p));
-    for (uint32_t i = threadIdx.x; i < p.n_cycles; i += blockDim.x) s_len[i] = p.cycle_len[i];
-    __syncthreads();
+    if constexpr (kShared) {
+        for (uint32_t i = threadIdx.x; i < p.total_len; i += blockDim.x)
+            sm_off[i] = static_cast<Off>(local_offset(p.cycles[i], p));
+        for (uint32_t i = threadIdx.x; i < p.n_cycles; i += blockDim.x) s_len[i] = p.cycle_len[i];
+        __syncthreads();
+    }
     double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -426,19 +429,22 @@ __global__ void __launch_bounds__(kThreads) k_perm(double2* __restrict__ st, PPe
         double2* __restrict__ sg = s + (expand_bits(g, p.fixed) | p.cmask);
         uint32_t start = 0;
         for (uint32_t c = 0; c < p.n_cycles; ++c) {
-            const uint32_t len = s_len[c];
-            const Off* off = sm_off + start;
-            const double2 last = sg[off[len - 1]];
+            const uint32_t len = kShared ? s_len[c] : p.cycle_len[c];
+            auto off = [&](uint32_t i) -> uint64_t {
+                if constexpr (kShared) return sm_off[start + i];
+                else return local_offset(p.cycles[start + i], p);
+            };
+            const double2 last = sg[off(len - 1)];
             uint32_t i = len - 1;
             for (; i >= 8; i -= 8) {
                 double2 t[8];
 #pragma unroll
-                for (uint32_t u = 0; u < 8; ++u) t[u] = sg[off[i - 1 - u]];
+                for (uint32_t u = 0; u < 8; ++u) t[u] = sg[off(i - 1 - u)];
 #pragma unroll
-                for (uint32_t u = 0; u < 8; ++u) sg[off[i - u]] = t[u];
+                for (uint32_t u = 0; u < 8; ++u) sg[off(i - u)] = t[u];
             }
-            for (; i > 0; --i) sg[off[i]] = sg[off[i - 1]];
-            sg[off[0]] = last;
+            for (; i > 0; --i) sg[off(i)] = sg[off(i - 1)];
+            sg[off(0)] = last;
             start += len;
         }
     }
@@ -470,16 +476,18 @@ void launch_perm(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
     const size_t smem = (narrow ? sizeof(uint32_t) : sizeof(uint64_t)) * total_len +
                         sizeof(uint32_t) * n_cycles;
     dim3 grid(grid_for(ctx, p.n_groups), batch);
-    if (narrow) {
+    if (smem > 160 * 1024) {
+        k_perm<uint64_t, false><<<grid, kThreads, 0, ctx.stream>>>(st, p);
+    } else if (narrow) {
         if (smem > 48 * 1024)
-            cudaFuncSetAttribute(k_perm<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_perm<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem));
-        k_perm<uint32_t><<<grid, kThreads, smem, ctx.stream>>>(st, p);
+        k_perm<uint32_t, true><<<grid, kThreads, smem, ctx.stream>>>(st, p);
     } else {
         if (smem > 48 * 1024)
-            cudaFuncSetAttribute(k_perm<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_perm<uint64_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem));
-        k_perm<uint64_t><<<grid, kThreads, smem, ctx.stream>>>(st, p);
+        k_perm<uint64_t, true><<<grid, kThreads, smem, ctx.stream>>>(st, p);
     }
     check_launch("perm");
 }

@@ -95,6 +95,28 @@ def test_diagonal_only_passes(port, n):
     assert np.max(np.abs(sv.to_numpy() - want)) < TOL
 
 
+@pytest.mark.parametrize("k,controls", [(12, 0), (15, 0), (16, 0), (15, 1)])
+def test_wide_permutations(port, k, controls):
+    """Permutation tables of 2^12..2^16 entries, plain and controlled: the widest ones
+    exceed shared memory and take the kernel's global-table form."""
+    n = 17
+    rng = np.random.default_rng(k + controls)
+    init = W.gaussian_state(n, seed=k)
+    qubits = [int(q) for q in rng.permutation(n)[: k + controls]]
+    table = [int(v) for v in rng.permutation(1 << k)]
+    qc = lq.QuantumCircuit(n)
+    if controls:
+        from litequantumcomputingsimulator_b200.circuit import Gate, GateType, Instruction
+        qc.append(Instruction(Gate(GateType.Permutation, [], controls, [], table), qubits))
+    else:
+        qc.permutation(table, qubits)
+    qc.h(0)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    sv = lq.Statevector.from_numpy(init)
+    sv.apply(qc, fuse_gates=False)
+    assert np.max(np.abs(sv.to_numpy() - want)) < TOL
+
+
 def test_state_too_large_fails_cleanly():
     with pytest.raises((MemoryError, ValueError)):
         lq.Statevector(38)   # 4 TiB
