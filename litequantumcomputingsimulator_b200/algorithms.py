@@ -371,9 +371,7 @@ def shor(N: int, shots: int = 64, max_attempts: int = 10,
         res.success, res.factor1, res.factor2 = True, min(b, N // b), max(b, N // b)
         return res
     n_work = N.bit_length()
-    n_count = 2 * n_work
-    if n_count + n_work > 30:
-        raise ValueError("shor: N needs more than 30 qubits")
+    n_count = 2 * n_work   # 3 * bit_length(N) qubits: up to N < 2^11 (33 qubits) on one B200
     count_dim = 1 << n_count
     rng = _Mt64Stream(seed if seed is not None else int.from_bytes(np.random.bytes(8), "little"))
     for attempt in range(max_attempts):
