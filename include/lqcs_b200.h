@@ -456,7 +456,7 @@ int lqcs_rng_uniforms(uint64_t seed, uint64_t count, double* out);
 
 /* Raw 64-bit draws `skip` .. `skip + count - 1` of std::mt19937_64 seeded with `seed` (the
  * engine behind lqcs::Rng, include/lqcs/core/random.hpp): what algorithms::shor
- * (src/algorithms/shor.cpp:77-111) draws its bases and simulator seeds from. */
+ * (src/algorithms/shor.cpp:72-102) draws its bases and simulator seeds from. */
 int lqcs_rng_u64(uint64_t seed, uint64_t skip, uint64_t count, uint64_t* out);
 
 /* ------------------------------------------------------------------ diagnostics */

@@ -201,7 +201,7 @@ def pow_mod(base: int, exp: int, mod: int) -> int:
 
 
 def is_prime(n: int) -> bool:
-    """Trial division by odd numbers up to sqrt(n) (number_theory.cpp:45-52)."""
+    """Trial division by odd numbers up to sqrt(n) (src/algorithms/number_theory.cpp:44-51)."""
     if n < 2:
         return False
     if n % 2 == 0:
@@ -215,9 +215,10 @@ def is_prime(n: int) -> bool:
 
 
 def perfect_power_base(n: int) -> int:
-    """b if n = b^k for some k >= 2 (the smallest such k), else 0 (number_theory.cpp:54-72:
-    k from 2 while 2^k <= n; the reference rounds a floating k-th root and checks its
-    neighbours, which for n < 2^53 finds the same b as the exact integer root used here)."""
+    """b if n = b^k for some k >= 2 (the smallest such k), else 0
+    (src/algorithms/number_theory.cpp:53-70: k from 2 while 2^k <= n; the reference rounds a
+    floating k-th root and checks its neighbours, which for n < 2^53 finds the same b as the
+    exact integer root used here)."""
     if n < 4:
         return 0
     k = 2
@@ -245,7 +246,7 @@ def _iroot(n: int, k: int) -> int:
 def continued_fraction_denominators(num: int, den: int, max_denominator: int) -> list:
     """Denominators q_i = a_i q_{i-1} + q_{i-2} (q_{-1} = 0, q_{-2} = 1) of the convergents
     of num/den, stopping before the first one above max_denominator
-    (number_theory.cpp:74-92)."""
+    (src/algorithms/number_theory.cpp:72-89)."""
     out = []
     km1, km2 = 0, 1
     while den != 0:
@@ -263,7 +264,7 @@ def continued_fraction_denominators(num: int, den: int, max_denominator: int) ->
 
 def modular_exponentiation(a: int, N: int, n_counting: int, n_work: int) -> QuantumCircuit:
     """|c>|y> -> |c>|a^c y mod N> on counting register [0, n_counting) and work register
-    [n_counting, n_counting + n_work) (src/algorithms/arithmetic.cpp:10-42): one singly
+    [n_counting, n_counting + n_work) (src/algorithms/arithmetic.cpp:10-43): one singly
     controlled permutation per counting qubit j, y -> a^(2^j) y mod N for y < N and the
     identity on y >= N.  The engine applies each as a controlled permutation of the work
     register (cycles in shared memory)."""
@@ -334,7 +335,7 @@ class ShorResult:
 
 
 def _try_period(N: int, a: int, r: int, res: ShorResult) -> bool:
-    """Factors from a candidate period r (shor.cpp:21-40)."""
+    """Factors from a candidate period r (src/algorithms/shor.cpp:22-39)."""
     if r == 0 or r >= N or pow(a, r, N) != 1 or r % 2 != 0:
         return False
     x = pow(a, r // 2, N)
@@ -350,7 +351,7 @@ def _try_period(N: int, a: int, r: int, res: ShorResult) -> bool:
 
 def shor(N: int, shots: int = 64, max_attempts: int = 10,
          seed: Optional[int] = None) -> ShorResult:
-    """Shor's factoring (src/algorithms/shor.cpp:44-129): classical shortcuts (even N, prime
+    """Shor's factoring (src/algorithms/shor.cpp:43-129): classical shortcuts (even N, prime
     N, perfect powers, a lucky gcd), then per attempt a base a drawn from lqcs::Rng(seed),
     period finding on the GPU (H on 2w counting qubits, the controlled modular
     multiplications, inverse QFT, `shots` measurements with a simulator seeded by the next
