@@ -82,6 +82,8 @@ SHOR = {
     "shor_35": {"N": 35, "shots": 64, "max_attempts": 10, "seed": 7},
     "shor_55": {"N": 55, "shots": 64, "max_attempts": 10, "seed": 7},
     "shor_91": {"N": 91, "shots": 128, "max_attempts": 10, "seed": 3},
+    # 24 qubits: the reference takes about 2.5 minutes on 8 cores (per-shot sampling)
+    "shor_221": {"N": 221, "shots": 64, "max_attempts": 10, "seed": 4},
     "shor_21_gcd": {"N": 21, "shots": 64, "max_attempts": 10, "seed": 7},
     "shor_27_power": {"N": 27, "shots": 64, "max_attempts": 10, "seed": 1},
     "shor_97_prime": {"N": 97, "shots": 64, "max_attempts": 10, "seed": 1},
