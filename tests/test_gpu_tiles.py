@@ -116,6 +116,21 @@ def test_diagonal_runs_and_gated_phases(port, tile_env, n, reg):
     assert np.max(np.abs(run(q, TILE, init) - want)) < TOL
 
 
+@pytest.mark.parametrize("n,k", [(24, 20), (24, 16), (22, 19)])
+def test_partial_inverse_qft_on_larger_state(n, k):
+    """The inverse QFT of k of n qubits through register tile passes equals gate-by-gate
+    application (a missing barrier between tiles once made (24, 20) wrong by ~1e-3)."""
+    init = W.gaussian_state(n, seed=n + k)
+    qc = lq.QuantumCircuit(n)
+    qc.compose(lq.algorithms.qft_inverse(k))
+    a = lq.Statevector.from_numpy(init)
+    a.apply(qc, fuse_gates=False)
+    for _ in range(2):
+        b = lq.Statevector.from_numpy(init)
+        b.apply(qc, fuse_gates=True, fusion_mode=TILE)
+        assert np.max(np.abs(a.to_numpy() - b.to_numpy())) < TOL
+
+
 @pytest.mark.parametrize("n", [12, 15])
 def test_relabelled_swaps(port, tile_env, n):
     """SWAPs of two tile qubits become relabellings in register passes (the store writes
