@@ -54,6 +54,8 @@ def parse():
                          "default all")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-sharded", action="store_true",
+                    help="skip the sharded batched-axis leg (parameter sets, trajectory shots)")
     return ap.parse_args()
 
 
@@ -146,10 +148,26 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ distributed plumbing
+def relaunch_under_torchrun(gpus: int) -> int:
+    """`bench.py --gpus N` (N > 1) started without a launcher: start N ranks on this node
+    with torch.distributed.run (rendezvous on 127.0.0.1) and return their exit status."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py")] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def dist_setup(gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but WORLD_SIZE is {world}; launch with "
+                         f"torchrun --nproc-per-node {gpus} or without a launcher")
     if world > 1:
         import torch
         import torch.distributed as dist
@@ -175,13 +193,35 @@ def barrier(dist):
 
 
 # ------------------------------------------------------------------ reference arm
+def reference_layer_sample(ref, n: int, depth: int, seed: int, steps: int, warmup: int):
+    """Time the reference's OpenMP kernels (oracle/_ref) on whole brickwork layers: step s
+    applies layer s mod depth (n U gates then n // 2 CX, 45 gates at 30 qubits) to one
+    pre-touched 2^n-amplitude host state; each warm-up step applies one gate (the state's
+    allocation and first touch happen before them).  Returns (seconds per timed step,
+    algorithmic bytes per step, the time of the whole depth-`depth` circuit extrapolated
+    from the mean layer time)."""
+    from oracle import workload as OW
+    qc = OW.brickwork(n, depth, seed)
+    per = OW.layer_size(n)
+    layers = [qc.slice(l * per, (l + 1) * per) for l in range(depth)]
+    for w in range(warmup):
+        ref.time_apply(qc.slice(w % len(qc), w % len(qc) + 1), 1)
+    times, nbytes = [], []
+    for s in range(steps):
+        lay = layers[s % depth]
+        times.append(ref.time_apply(lay, 1))
+        nbytes.append(lay.alg_bytes())
+    mean_layer = sum(times) / len(times)
+    return times, nbytes, mean_layer * depth, qc
+
+
 def reference_arm(args):
-    """The reference's own OpenMP CPU implementation (oracle/_ref) on this host's cores,
-    on a bounded sample of the same workload: each step applies the first G gates of the
-    30-qubit brickwork circuit to a 16 GiB host state (G sized so a step takes ~3 s)."""
+    """The reference's own OpenMP CPU implementation (oracle/_ref, compiled from the
+    reference's sources) on this host's cores, on the engine arm's workload: the seeded
+    30-qubit brickwork of depth 40, one whole layer (45 gates, 1/40 of the circuit) per
+    timed step on a 16 GiB host state.  Builds its records and angles with the oracle alone
+    (the reference's own lqcs::Rng through the same library), so no engine code is loaded."""
     from oracle.oracle import Ref
-    import litequantumcomputingsimulator_b200 as lq
-    from litequantumcomputingsimulator_b200 import workloads as W
     if not Ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liblqcs_ref.so was not built"}))
         return 0
@@ -189,36 +229,29 @@ def reference_arm(args):
     cores = os.cpu_count() or 1
     ref.set_threads(cores)
     n = args.qubits
-    qc = W.brickwork(n, args.depth, args.seed)
-    insts = qc.instructions()
-    # size the sample: time one gate first
-    one = lq.QuantumCircuit(n)
-    one.append(insts[0])
     try:
-        t1 = ref.time_apply(one, 1)
+        times, nbytes, full_s, qc = reference_layer_sample(ref, n, args.depth, args.seed,
+                                                           args.steps, args.warmup)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference could not run: {e}"}))
         return 0
-    g = max(1, min(len(insts), int(3.0 / max(t1, 1e-3))))
-    sample = lq.QuantumCircuit(n)
-    for inst in insts[:g]:
-        sample.append(inst)
-    nbytes = W.alg_bytes(sample)
-    for _ in range(args.warmup):
-        ref.time_apply(sample, 1)
-    times = [ref.time_apply(sample, 1) for _ in range(args.steps)]
     total = sum(times)
-    value = nbytes * args.steps / total / 1e9
+    value = sum(nbytes) / total / 1e9
+    sample = (f"one whole brickwork layer per timed step ({n} U + {n // 2} CX of the {len(qc)}-gate "
+              f"circuit, layers 0..{min(args.steps, args.depth) - 1}), reference OpenMP kernels on "
+              f"a pre-touched host state; warm-up steps apply one gate each")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (seeded brickwork)",
-        "config": {"workload": f"brickwork n={n} depth={args.depth} seed={args.seed}",
-                   "sample": f"first {g} of {len(insts)} gates per step", "l2": "state > L2"},
+        "config": {"workload": f"brickwork n={n} depth={args.depth} seed={args.seed} ({len(qc)} gates)",
+                   "sample": sample,
+                   "extrapolated_full_circuit_s": full_s,
+                   "extrapolation": f"mean layer time x {args.depth} layers",
+                   "l2": "state > L2"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"first {g} gates of the {n}-qubit brickwork circuit per step, "
-                                   "OpenMP kernels of the reference on a pre-touched host state"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -272,29 +305,24 @@ def cpu_side_baselines(ref) -> dict:
     return out
 
 
-def cpu_baseline(n: int, qc, budget_s: float = 12.0) -> dict:
+def cpu_baseline(n: int, qc, depth: int, seed: int, budget_s: float = 12.0) -> dict:
     from oracle.oracle import Ref, Port
     import litequantumcomputingsimulator_b200 as lq
     from litequantumcomputingsimulator_b200 import workloads as W
-    insts = qc.instructions()
     if Ref.available():
         ref = Ref()
         cores = os.cpu_count() or 1
         ref.set_threads(cores)
-        one = lq.QuantumCircuit(n)
-        one.append(insts[0])
-        t1 = ref.time_apply(one, 1)
-        g = max(1, min(len(insts), int(budget_s / max(t1, 1e-3))))
-        sample = lq.QuantumCircuit(n)
-        for inst in insts[:g]:
-            sample.append(inst)
-        t = ref.time_apply(sample, 1)
-        out = {"value": W.alg_bytes(sample) / t / 1e9, "unit": UNIT, "cores": cores,
+        times, nbytes, full_s, _qc = reference_layer_sample(ref, n, depth, seed, 1, 1)
+        t = times[0]
+        out = {"value": nbytes[0] / t / 1e9, "unit": UNIT, "cores": cores,
                "kind": "reference",
-               "sample": f"first {g} gates of the {n}-qubit brickwork, reference OpenMP kernels, "
-                         f"{t:.2f} s"}
+               "sample": f"brickwork layer 0 of the {n}-qubit circuit ({n} U + {n // 2} CX), "
+                         f"reference OpenMP kernels on a pre-touched host state, {t:.2f} s; "
+                         f"whole circuit extrapolated {full_s:.0f} s"}
         out.update(cpu_side_baselines(ref))
         return out
+    insts = qc.instructions()
     # the scalar port on a 26-qubit sample, one core
     m = min(n, 26)
     port = Port()
@@ -325,6 +353,8 @@ def main():
             return 0
         return reference_arm(args)
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_under_torchrun(args.gpus)
     rank, world, local, dist = dist_setup(args.gpus)
     import torch
     torch.cuda.set_device(local)
@@ -419,10 +449,15 @@ def main():
     if not args.no_e2e:
         e2e = run_e2e(lq, qc, gate_bytes, args, dist, device, world)
 
+    # ---- the batched axes sharded over the ranks (every N, weak scaling)
+    sharded = None
+    if not args.no_sharded:
+        sharded = run_sharded(lq, W, dist, device, world)
+
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
         try:
-            cpu = cpu_baseline(n, qc)
+            cpu = cpu_baseline(n, qc, depth, args.seed)
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -442,6 +477,7 @@ def main():
             "clocks": clock_info,
             "roofline": roofline,
             "e2e": e2e,
+            "sharded": sharded,
             "cpu_baseline": cpu,
             "extras": extras,
         }
@@ -449,6 +485,70 @@ def main():
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def run_sharded(lq, W, dist, device, world) -> dict:
+    """The two batched axes split over the ranks, each rank on its own GPU with no exchange
+    while it computes and one NCCL all-gather at the end (sharding.py): 256 parameter sets
+    per rank of the 16-qubit adjoint-gradient workload (200 rp gates, 500 terms), and 64
+    trajectory shots per rank of the 26-qubit noisy brickwork (depth 20, config-3 rates),
+    the ranks taking consecutive shot ranges of one seeded run.  Times are host-timed around
+    the synchronous calls plus the gather, max over ranks; rates count all ranks' work."""
+    import torch
+    from litequantumcomputingsimulator_b200 import sharding as SH
+    out = {"ranks": world}
+    group = None
+    if dist is None:   # one rank: the same workloads without the gather
+        return out | _sharded_single(lq, W)
+    pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+    ham = W.random_hamiltonian(16, 500, seed=12)
+    sets = W.random_parameter_sets(pc.num_parameters(), 256 * world, seed=13)
+    SH.sharded_adjoint_gradient(ham, pc, sets[: 2 * world], group=group)   # plan + graph
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    e, g = SH.sharded_adjoint_gradient(ham, pc, sets, group=group)
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, dist, device)
+    out["adjoint_sets"] = int(sets.shape[0])
+    out["adjoint_sets_per_s"] = sets.shape[0] / dt
+    out["adjoint_gradient_checksum"] = float(np.sum(g))
+    tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+    sim = lq.StatevectorSimulator(seed=404, max_resident=64)
+    sim.run_registers(W.brickwork(12, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3)), 8)
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    regs = SH.sharded_run_registers(sim, tq, 64 * world, group=group)
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, dist, device)
+    out["trajectory_shots"] = int(regs.size)
+    out["trajectories_per_s"] = regs.size / dt
+    out["trajectory_register_checksum"] = int(np.bitwise_xor.reduce(regs)) if regs.size else 0
+    return out
+
+
+def _sharded_single(lq, W) -> dict:
+    """The sharded leg's two workloads on one rank (256 sets, 64 shots), for the per-N rate."""
+    import torch
+    pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+    ham = W.random_hamiltonian(16, 500, seed=12)
+    sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
+    lq.algorithms.adjoint_gradient(ham, pc, sets[:2])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _e, g = lq.algorithms.adjoint_gradient(ham, pc, sets)
+    out = {"adjoint_sets": 256, "adjoint_sets_per_s": 256 / (time.perf_counter() - t0),
+           "adjoint_gradient_checksum": float(np.sum(g))}
+    tq = W.brickwork(26, 20, seed=303, measure=True, noise=(1e-3, 1e-2, 1e-3))
+    sim = lq.StatevectorSimulator(seed=404, max_resident=64)
+    sim.run_registers(W.brickwork(12, 2, seed=1, measure=True, noise=(1e-3, 1e-2, 1e-3)), 8)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    regs = sim.run_registers(tq, 64)
+    out.update({"trajectory_shots": 64, "trajectories_per_s": 64 / (time.perf_counter() - t0),
+                "trajectory_register_checksum": int(np.bitwise_xor.reduce(regs))})
+    return out
 
 
 def run_e2e(lq, qc, gate_bytes, args, dist=None, device=None, world=1):
@@ -479,6 +579,15 @@ def run_e2e(lq, qc, gate_bytes, args, dist=None, device=None, world=1):
     return {"value": world * gate_bytes / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(16 << n), "s_per_step": dt, "pinned": pinned,
             "path": "StatevectorSimulator.run_statevector + Statevector.to_numpy (D2H)"}
+
+
+def device_maxdiff(a, b, chunk: int = 1 << 26) -> float:
+    """max |a_i - b_i| of two device states, in chunks (no full-size temporaries)."""
+    ta, tb = a.to_torch(), b.to_torch()
+    worst = 0.0
+    for lo in range(0, ta.numel(), chunk):
+        worst = max(worst, (ta[lo:lo + chunk] - tb[lo:lo + chunk]).abs().max().item())
+    return worst
 
 
 def run_extras(lq, W, N, n, sv, hbm_peak, args):
@@ -702,22 +811,32 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
             out["costmodel_collect_train_s"] = time.perf_counter() - t0
             held = W.random_mix_circuit(32, 16, seed=777)
             big = lq.Statevector(32)
-            res = {}
+            first = lq.Statevector(32)   # the greedy plan's result, for the amplitude check
+            res, diffs = {}, {}
             for name, mode in (("greedy", CM.GREEDY), ("learned", CM.LEARNED), ("default", 0)):
                 prog = lq.simulator.CompiledCircuit(held, True, 0, mode)
+                N.call("lqcs_state_set_zero", big.handle)
+                torch.cuda.synchronize()
                 s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s.record()
                 prog.apply(big)
                 e.record()
                 torch.cuda.synchronize()
                 res[name] = (s.elapsed_time(e), prog.n_ops)
+                if name == "greedy":
+                    first.to_torch().copy_(big.to_torch())
+                else:
+                    diffs[name] = device_maxdiff(big, first)
             out["costmodel_32q_greedy_ms"] = res["greedy"][0]
             out["costmodel_32q_learned_ms"] = res["learned"][0]
             out["costmodel_32q_default_ms"] = res["default"][0]
             out["costmodel_32q_ops"] = {k: v[1] for k, v in res.items()}
             out["costmodel_32q_speedup"] = res["greedy"][0] / res["learned"][0]
-            del big
+            out["costmodel_32q_max_amp_diff_vs_greedy"] = diffs
+            del big, first
             torch.cuda.empty_cache()
+            if max(diffs.values()) > 1e-12:
+                raise AssertionError(f"32-qubit plans disagree: max |d psi| {diffs}")
         except Exception as ex:  # noqa: BLE001
             out["costmodel_error"] = str(ex)
 

@@ -282,16 +282,18 @@ int lqcs_state_expectation_terms(const lqcs_state* st, const char* const* paulis
                                  double* per_term, double* total);
 
 /* <psi|P_t|psi> for up to LQCS_NOALLOC_MAX_TERMS Pauli strings, for callers that cannot
- * allocate device memory (an arena or pool that owns the device, a host callback inside a
- * CUDA graph, an embedding that forbids cudaMalloc after start-up).  Allocates nothing:
- * the caller passes the amplitudes (2^n_qubits complex128 in device memory, laid out as
- * above) and a host array of n_terms doubles; the partial sums live in one static device
- * array of 131,200 bytes inside the library, held by every GPU that loads it until exit.
- * More than LQCS_NOALLOC_MAX_TERMS terms -> LQCS_ERR_INVALID_ARGUMENT.  The first call on
- * a device looks up the array's device address, so make it before any stream capture on
- * that device.  All calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  Waits for completion on `stream` (NULL = default stream).
- * No counterpart in the reference. */
+ * allocate device memory (an arena or pool that owns the device, an embedding that forbids
+ * cudaMalloc after start-up).  Allocates nothing: the caller passes the amplitudes
+ * (2^n_qubits complex128 in device memory, laid out as above) and a host array of n_terms
+ * doubles; the partial sums live in one static device array of 131,200 bytes inside the
+ * library, held by every GPU that loads it until exit.  More than LQCS_NOALLOC_MAX_TERMS
+ * terms -> LQCS_ERR_INVALID_ARGUMENT.  An ordinary host call: it launches kernels and waits
+ * for `stream` (NULL = default stream), so it must not run inside stream capture or in a
+ * CUDA host function (cudaLaunchHostFunc, graph host nodes), where CUDA calls are not
+ * allowed.  The first call on a device looks up the array's device address (with that
+ * device current) and keeps it; after a cudaDeviceReset call lqcs_release_caches, which
+ * forgets it.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  No counterpart in the reference. */
 enum { LQCS_NOALLOC_MAX_TERMS = 16 };
 int lqcs_expectation_terms_noalloc(const void* d_amps, uint32_t n_qubits,
                                    const char* const* paulis, uint64_t n_terms,

@@ -434,6 +434,7 @@ int lqcs_release_caches(void) {
         lqcs_b200::clear_autotune_cache();
         lqcs_b200::clear_program_cache();
         lqcs_b200::clear_state_pool();
+        lqcs_b200::forget_static_scratch_addresses();
     });
 }
 

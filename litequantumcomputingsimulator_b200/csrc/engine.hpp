@@ -187,6 +187,7 @@ void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, doub
 
 // Expectation values with the scratch in a static device array (static_expect.cu).
 uint32_t static_expectation_max_terms();
+void forget_static_scratch_addresses();   // after a device reset (lqcs_release_caches)
 void expectation_terms_static(const void* d_amps, uint32_t n_qubits, const char* const* paulis,
                               uint64_t n_terms, double* host_values, cudaStream_t stream);
 

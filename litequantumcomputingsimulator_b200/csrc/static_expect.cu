@@ -2,22 +2,30 @@
 //
 // For callers that hold their amplitudes in device memory they manage themselves and may
 // not allocate more: code running inside a memory pool or arena that owns the whole
-// device, a CUDA-graph node's host callback, or an embedding that forbids cudaMalloc
-// after start-up.  The regular expectation path (lqcs_state_expectation_terms) needs a
-// state handle and scratch it allocates; this path uses a fixed scratch array that is
-// part of the library image instead.
+// device, or an embedding that forbids cudaMalloc after start-up.  The regular expectation
+// path (lqcs_state_expectation_terms) needs a state handle and scratch it allocates; this
+// path uses a fixed scratch array that is part of the library image instead.  It is an
+// ordinary host call: it launches kernels, copies the results to the host and waits for
+// its stream, so it must not be made inside stream capture or from a CUDA host function
+// (cudaLaunchHostFunc or a graph host node, where CUDA calls are not allowed).
 //
 // The scratch is one file-scope __device__ array of kStaticScratchDoubles doubles
 // (131,200 bytes).  Every GPU that loads the library holds its own copy until the process
 // exits.  Host code cannot use the array's name as a device address: on first use on a
 // device (with that device current) the address is fetched once with
-// cudaGetSymbolAddress, checked, cached per device, and passed to the kernels.  That
-// first call must therefore come before any stream capture on that device.
+// cudaGetSymbolAddress, checked, cached per device, and passed to the kernels.  A device
+// reset (cudaDeviceReset) invalidates that address: lqcs_release_caches forgets the
+// cached addresses, so call it after a reset, as for the library's other device caches.
 //
 // Every call shares the same array and leaves its last contents behind.  The partial
 // kernel overwrites every slot the final kernel reads, so nothing has to start at zero.
 // Calls whose work overlaps on the GPU (different streams, or different host threads
 // without ordering) race on the array and give wrong results; serialise them.
+//
+// The partial kernel reads, per amplitude, the partner a_{i ^ x_t} of every term: up to
+// 16 extra reads per amplitude, mostly from L1/L2 when the X masks are small.  The
+// regular path groups terms by X mask instead; with at most 16 terms and a fixed scratch
+// this simpler form is kept.
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -40,6 +48,15 @@ static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_addr[kMaxDevices] = {};
+
+}  // namespace
+
+void forget_static_scratch_addresses() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (double*& a : g_addr) a = nullptr;
+}
+
+namespace {
 
 double* scratch_address() {
     int dev = 0;

@@ -1,0 +1,188 @@
+"""Parity at the headline sizes (28-30 qubits) and at the full shape of the batched
+gradient workload.
+
+* 30 qubits: the seeded brickwork of depth 40 (1800 gates) and QFT(30) on a random
+  Gaussian state, through the default path (register tile passes with searched high
+  qubits), against the engine's own gate-by-gate path on a second 16 GiB state; compared on
+  the device in chunks.
+* 28 and 30 qubits against the reference compiled from its own sources: the first two
+  brickwork layers of the headline circuit (from |0..0>, `StatevectorSimulator::
+  run_statevector`, src/backend/statevector_simulator.cpp:222-230) and QFT(28) on a Gaussian
+  state (src/algorithms/qft.cpp:7-23, applied by the reference's kernels).  The 30-qubit
+  case holds three 16 GiB host arrays and runs only where the host has the memory.
+* 16 qubits, 200 Pauli rotations of weight 2..8, 500 Hamiltonian terms, 256 parameter sets
+  in one batched adjoint call: sets 0 and 255 against the reference's parameter-shift
+  gradient (src/algorithms/vqe.cpp:68-94) within 1e-9, energies within 1e-11, and ten
+  parameters against central differences (h = 1e-4) within 1e-6.
+* A QASM text written by the reference (io::to_qasm, src/io/qasm.cpp) read back and run
+  through the engine, against the reference's run_statevector of the same circuit.
+
+Tolerances: amplitudes 1e-12 absolute, as everywhere in these tests.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import litequantumcomputingsimulator_b200 as lq
+from litequantumcomputingsimulator_b200 import io as qio
+from litequantumcomputingsimulator_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+GATE_BY_GATE, TILE = 3, 4
+CHUNK = 1 << 26
+
+
+def _device_maxdiff(a: "lq.Statevector", b: "lq.Statevector") -> float:
+    ta, tb = a.to_torch(), b.to_torch()
+    worst = 0.0
+    for lo in range(0, ta.numel(), CHUNK):
+        d = (ta[lo:lo + CHUNK] - tb[lo:lo + CHUNK]).abs().max().item()
+        worst = max(worst, d)
+    return worst
+
+
+def _host_maxdiff(a: np.ndarray, b: np.ndarray) -> float:
+    worst = 0.0
+    for lo in range(0, a.size, CHUNK):
+        worst = max(worst, float(np.max(np.abs(a[lo:lo + CHUNK] - b[lo:lo + CHUNK]))))
+    return worst
+
+
+def _device_gaussian(sv: "lq.Statevector", seed: int) -> None:
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    t = sv.to_torch()
+    for lo in range(0, t.numel(), CHUNK):
+        t[lo:lo + CHUNK] = torch.randn(min(CHUNK, t.numel() - lo), dtype=torch.complex128,
+                                       device="cuda", generator=g)
+    t /= torch.linalg.vector_norm(t)
+
+
+def _host_bytes_available() -> int:
+    try:
+        import psutil
+        return int(psutil.virtual_memory().available)
+    except Exception:  # noqa: BLE001
+        return os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+
+
+@pytest.fixture
+def threads(ref):
+    ref.set_threads(os.cpu_count() or 1)
+    return ref
+
+
+def test_brickwork_30q_depth40_tile_passes_equal_gate_by_gate():
+    qc = W.brickwork(30, 40, seed=2025)
+    a = lq.Statevector(30)
+    lq.simulator.CompiledCircuit(qc, True, 0, 0).apply(a)
+    b = lq.Statevector(30)
+    lq.simulator.CompiledCircuit(qc, True, 0, GATE_BY_GATE).apply(b)
+    assert abs(a.norm() - 1.0) < 1e-10
+    assert _device_maxdiff(a, b) < TOL
+
+
+def test_qft30_on_gaussian_state_tile_passes_equal_gate_by_gate():
+    q = lq.algorithms.qft(30)
+    a = lq.Statevector(30)
+    _device_gaussian(a, seed=30)
+    b = lq.Statevector(30)
+    b.to_torch().copy_(a.to_torch())
+    lq.simulator.CompiledCircuit(q, True, 0, 0).apply(a)
+    lq.simulator.CompiledCircuit(q, True, 0, GATE_BY_GATE).apply(b)
+    assert _device_maxdiff(a, b) < TOL
+
+
+def _first_layers(n: int, depth: int, layers: int, seed: int) -> "lq.QuantumCircuit":
+    full = W.brickwork(n, depth, seed)
+    out = lq.QuantumCircuit(n)
+    for inst in full.instructions()[: layers * (n + n // 2)]:
+        out.append(inst)
+    return out
+
+
+def test_brickwork_28q_two_layers_vs_reference(threads):
+    qc = _first_layers(28, 40, 2, seed=2025)
+    want = threads.run_statevector(qc)
+    got = lq.StatevectorSimulator().run_statevector(qc).to_numpy()
+    assert _host_maxdiff(got, want) < TOL
+
+
+def test_brickwork_30q_two_layers_vs_reference(threads):
+    if _host_bytes_available() < (64 << 30):
+        pytest.skip("the 30-qubit reference comparison needs 64 GiB of free host memory")
+    qc = _first_layers(30, 40, 2, seed=2025)
+    got = lq.StatevectorSimulator().run_statevector(qc).to_numpy()
+    want = threads.run_statevector(qc)
+    assert _host_maxdiff(got, want) < TOL
+
+
+def test_qft28_on_gaussian_state_vs_reference(threads):
+    init = W.gaussian_state(28, seed=28)
+    q = lq.algorithms.qft(28)
+    want = threads.evolve_from(q, init)
+    sv = lq.Statevector.from_numpy(init)
+    lq.simulator.CompiledCircuit(q, True, 0, 0).apply(sv)
+    assert _host_maxdiff(sv.to_numpy(), want) < TOL
+
+
+def test_adjoint_full_config_shape_vs_reference(threads):
+    pc, _ = W.random_pauli_ansatz(16, 200, seed=11)
+    ham = W.random_hamiltonian(16, 500, seed=12)
+    sets = W.random_parameter_sets(pc.num_parameters(), 256, seed=13)
+    e, g = lq.algorithms.adjoint_gradient(ham, pc, sets)
+    assert e.shape == (256,) and g.shape == (256, 200)
+    for b in (0, 255):
+        want = threads.parameter_shift_gradient(ham, pc, sets[b])
+        assert np.max(np.abs(g[b] - want)) < 1e-9
+        e_ref = threads.expectation(threads.run_statevector(pc.bind(sets[b])), ham)
+        assert abs(e[b] - e_ref) < 1e-11
+    # central differences on ten parameters of set 0, energies from the batched forward pass
+    h = 1e-4
+    ks = list(range(0, 200, 20))
+    shifted = []
+    for k in ks:
+        for s in (h, -h):
+            p = sets[0].copy()
+            p[k] += s
+            shifted.append(p)
+    en = lq.algorithms.batched_energy(ham, pc, np.array(shifted))
+    for i, k in enumerate(ks):
+        fd = (en[2 * i] - en[2 * i + 1]) / (2 * h)
+        assert abs(g[0, k] - fd) < 1e-6
+
+
+def test_reference_written_qasm_runs_through_engine(threads):
+    rng = np.random.default_rng(17)
+    qc = lq.QuantumCircuit(12)
+    for _ in range(120):
+        a, b, c = (int(x) for x in rng.permutation(12)[:3])
+        k = int(rng.integers(8))
+        ang = float(rng.uniform(-math.pi, math.pi))
+        if k == 0:
+            qc.h(a)
+        elif k == 1:
+            qc.cx(a, b)
+        elif k == 2:
+            qc.u(ang, 0.5 * ang, -ang, a)
+        elif k == 3:
+            qc.cp(ang, a, b)
+        elif k == 4:
+            qc.ccx(a, b, c)
+        elif k == 5:
+            qc.swap(a, b)
+        elif k == 6:
+            qc.crz(ang, a, b)
+        else:
+            qc.rx(ang, a)
+    text = threads.qasm_roundtrip(qio.to_qasm(qc))   # written by the reference
+    parsed = qio.from_qasm(text)
+    want = threads.run_statevector(parsed)
+    for mode in (0, GATE_BY_GATE, TILE):
+        sv = lq.Statevector(12)
+        sv.apply(parsed, fuse_gates=True, fusion_mode=mode)
+        assert np.max(np.abs(sv.to_numpy() - want)) < TOL

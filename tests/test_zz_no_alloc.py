@@ -1,8 +1,9 @@
 """The allocation-free expectation entry point (lqcs_expectation_terms_noalloc).
 
 It exists for callers that cannot allocate device memory — code inside a pool or arena that
-owns the whole device, a host callback in a CUDA graph, an embedding that forbids cudaMalloc
-after start-up — and keeps its partial sums in a static device array of the library.  Its
+owns the whole device, an embedding that forbids cudaMalloc after start-up — and keeps its
+partial sums in a static device array of the library.  It is an ordinary host call (it waits
+for its stream), never one made inside stream capture or a CUDA host function.  Its
 results must equal those of the regular entry point (lqcs_state_expectation_terms) within
 the expectation tolerance of the other tests, on consecutive calls that reuse the array.
 This file is collected last so that a run stopping at the first failure has already run
