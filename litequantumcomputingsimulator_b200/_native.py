@@ -124,6 +124,10 @@ SIGNATURES = {
     "lqcs_last_error": (C.c_char_p, []),
     "lqcs_version": (C.c_char_p, []),
     "lqcs_kernel_launch_count": (C.c_uint64, []),
+    "lqcs_debug_emulate_register_passes": (C.c_int, [C.c_uint32, _P(Instruction), C.c_uint64,
+                                                     C.c_uint64, C.c_int32, C.c_void_p,
+                                                     C.c_uint64, _P(C.c_uint64), _P(C.c_uint64),
+                                                     C.c_char_p, C.c_uint64]),
     "lqcs_state_create": (C.c_int, [C.c_uint32, C.c_void_p, _P(StatePtr)]),
     "lqcs_state_create_batch": (C.c_int, [C.c_uint32, C.c_uint32, C.c_void_p, _P(StatePtr)]),
     "lqcs_state_destroy": (C.c_int, [StatePtr]),

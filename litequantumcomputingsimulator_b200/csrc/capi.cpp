@@ -64,6 +64,30 @@ const char* lqcs_version(void) { return "lqcs_b200 0.1.0 sm_100a"; }
 
 uint64_t lqcs_kernel_launch_count(void) { return lqcs_b200::launch_count(); }
 
+int lqcs_debug_emulate_register_passes(uint32_t n_qubits, const lqcs_instruction* insts,
+                                       uint64_t n_insts, uint64_t grid, int32_t sync_tiles,
+                                       double* state, uint64_t race_ctas, uint64_t* n_passes,
+                                       uint64_t* n_races, char* report, uint64_t report_cap) {
+    return guarded([&] {
+        need(n_passes, "n_passes");
+        need(n_races, "n_races");
+        if (n_qubits < lqcs_b200::kRegMinBits || n_qubits > 26)
+            lqcs_b200::invalid("register tile emulation: n_qubits must be in [9, 26]");
+        if (sync_tiles < 0 || sync_tiles > 3)
+            lqcs_b200::invalid("register tile emulation: sync_tiles must be 0, 1, 2 or 3");
+        std::string first;
+        lqcs_b200::emulate_register_program(n_qubits, insts, n_insts, grid,
+                                            sync_tiles == 3 ? 1 : sync_tiles, sync_tiles == 3,
+                                            reinterpret_cast<lqcs_b200::cd*>(state), race_ctas,
+                                            n_passes, n_races, &first);
+        if (report && report_cap) {
+            const size_t k = std::min<size_t>(first.size(), report_cap - 1);
+            std::memcpy(report, first.data(), k);
+            report[k] = 0;
+        }
+    });
+}
+
 int lqcs_state_create(uint32_t n_qubits, void* stream, lqcs_state** out) {
     return guarded([&] {
         need(out, "out");

@@ -186,6 +186,14 @@ double kraus_probability(lqcs_state& st, uint32_t q, const std::array<cd, 4>& k)
 void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, double* min_margin);
 
 // Expectation values with the scratch in a static device array (static_expect.cu).
+// Host emulation of the register tile kernel (reg_emulate.cpp).  sync_tiles: 1 barrier
+// between tiles, 0 none, 2 where a remap changes the warp bits (RegPass::cta_remaps).
+// pipe: the double-buffered kernel's access pattern (tile sizes 2^11 and 2^12).
+void emulate_register_program(uint32_t n, const lqcs_instruction* insts, uint64_t n_insts,
+                              uint64_t grid, int sync_tiles, bool pipe, cd* state,
+                              uint64_t race_ctas, uint64_t* n_passes, uint64_t* n_races,
+                              std::string* report);
+
 uint32_t static_expectation_max_terms();
 void forget_static_scratch_addresses();   // after a device reset (lqcs_release_caches)
 void expectation_terms_static(const void* d_amps, uint32_t n_qubits, const char* const* paulis,

@@ -460,6 +460,223 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     }
 }
 
+// ------------------------------------------------------------------ double-buffered passes
+//
+// The same pass with the next tile's HBM read overlapped with this tile's compute: each
+// thread issues cp.async copies of 16 of the next tile's amplitudes into the second of two
+// shared tile buffers while the CTA works on the first, and waits for them only when it
+// reaches that tile.  The tile arrives in shared memory in linear order (position q of the
+// tile at index q; thread t copies positions j * T + t, so a warp's copy is one coalesced
+// 512-byte row), is read into registers through layout 0, and the same buffer then serves
+// the remaps (swizzled slots).  One barrier per tile makes the copies visible, ends every
+// warp's use of the previous tile's buffer (which the next copies overwrite) and publishes
+// the per-tile diagonal tables.
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <int M, int MINB>
+__global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
+k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
+               const RegLayout* __restrict__ layouts, const double2* __restrict__ mats) {
+    constexpr uint32_t kT = 1u << (M - kRegBits);
+    constexpr uint32_t kTB = M - kRegBits;
+    constexpr uint32_t kN = 1u << M;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* bufs = reinterpret_cast<double2*>(smem);   // two tiles
+    double2* smat = bufs + 2 * kN;
+    RegOp* sops = reinterpret_cast<RegOp*>(smat + p.n_mat);
+    RegLayout* slay = reinterpret_cast<RegLayout*>(sops + p.n_ops);
+    double2* sdyn = reinterpret_cast<double2*>(
+        (reinterpret_cast<uintptr_t>(slay + p.n_layouts) + 15u) & ~uintptr_t{15});
+    __shared__ uint64_t gbit[kRegMaxBits];
+    __shared__ uint64_t sgbit[kRegMaxBits];
+    __shared__ uint32_t shbits[kTileMaxHigh];
+    __shared__ uint32_t sdynrec[kRegMaxDyn];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (uint32_t i = 0; i < kTileMaxHigh; ++i) shbits[i] = p.hbits[i];
+#pragma unroll
+        for (uint32_t i = 0; i < kRegMaxDyn; ++i) sdynrec[i] = p.dyn_rec[i];
+        for (uint32_t b = 0; b < M; ++b)
+            gbit[b] = uint64_t{1} << (b < p.L ? b : shbits[b - p.L]);
+        if (p.relabel) {
+#pragma unroll
+            for (uint32_t b = 0; b < kRegMaxBits; ++b)
+                if (b < M) sgbit[b] = uint64_t{1} << p.store_qubit[b];
+        }
+    }
+    const uint64_t* __restrict__ stbit = p.relabel ? sgbit : gbit;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(
+            mats + static_cast<uint64_t>(blockIdx.y) * p.mat_stride);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(smat);
+        for (uint32_t w = threadIdx.x; w < p.n_mat * 4u; w += kT) dst[w] = src[w];
+        src = reinterpret_cast<const uint32_t*>(ops);
+        dst = reinterpret_cast<uint32_t*>(sops);
+        for (uint32_t w = threadIdx.x; w < p.n_ops * (sizeof(RegOp) / 4); w += kT) dst[w] = src[w];
+        src = reinterpret_cast<const uint32_t*>(layouts);
+        dst = reinterpret_cast<uint32_t*>(slay);
+        for (uint32_t w = threadIdx.x; w < p.n_layouts * (sizeof(RegLayout) / 4); w += kT)
+            dst[w] = src[w];
+    }
+    __syncthreads();
+    const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
+    const uint32_t sdyn_addr = static_cast<uint32_t>(__cvta_generic_to_shared(sdyn));
+    const uint32_t bufs_addr = static_cast<uint32_t>(__cvta_generic_to_shared(bufs));
+    double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
+    // copy positions q = j * kT + t: tile bits 0..kTB-1 from t, the 4 above from j
+    uint64_t toff = 0;
+    for (uint32_t b = 0; b < kTB; ++b)
+        if ((threadIdx.x >> b) & 1u) toff |= gbit[b];
+    const uint64_t jb0 = gbit[kTB], jb1 = gbit[kTB + 1], jb2 = gbit[kTB + 2], jb3 = gbit[kTB + 3];
+    auto tile_base = [&](uint64_t tile) {
+        uint64_t b = tile << p.L;
+        for (uint32_t i = 0; i < p.h; ++i) b = insert_zero_bit(b, shbits[i]);
+        return b;
+    };
+    auto issue = [&](uint64_t tile, uint32_t which) {
+        const uint64_t g = tile_base(tile) | toff;
+        const uint32_t dst = bufs_addr + 16u * (which * kN + threadIdx.x);
+#pragma unroll
+        for (int j = 0; j < kE; ++j)
+            cp_async16(dst + 16u * kT * j, s + (g | ((j & 1) ? jb0 : 0) | ((j & 2) ? jb1 : 0) |
+                                               ((j & 4) ? jb2 : 0) | ((j & 8) ? jb3 : 0)));
+        cp_async_commit();
+    };
+    if (blockIdx.x < p.n_tiles) issue(blockIdx.x, 0);
+    uint32_t parity = 0;
+    for (uint64_t tid = blockIdx.x; tid < p.n_tiles; tid += gridDim.x, parity ^= 1u) {
+        const uint64_t base = tile_base(tid);
+        // this tile's diagonal tables: their parity's previous user (two tiles back) is done,
+        // since every warp passed the previous tile's barrier
+        const uint32_t dyn_base = parity * p.dyn_entries;
+        if (p.n_dyn) {
+            for (uint32_t w = threadIdx.x; w < p.n_dyn * 64u; w += kT) {
+                const RegOp& op = sops[sdynrec[w >> 6]];
+                const uint32_t e = w & 63u;
+                if (e >= (1u << op.k)) continue;
+                const double2* src = smat + op.mat_off;
+                double2 acc = src[e];
+                const double2* term = src + (1u << op.k);
+                for (uint32_t t = 0; t < op.nterm; ++t) {
+                    const double2 meta = term[2 * t + 1];
+                    const uint64_t hi = static_cast<uint64_t>(meta.y);
+                    const uint64_t gc = static_cast<uint64_t>(meta.x) | ((hi >> 6) << 32);
+                    const uint32_t em = static_cast<uint32_t>(hi & 63u);
+                    if ((base & gc) == gc && (e & em) == em) acc = cmul(term[2 * t], acc);
+                }
+                sdyn[dyn_base + op.dyn_off + e] = acc;
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (tid + gridDim.x < p.n_tiles) issue(tid + gridDim.x, parity ^ 1u);
+        double2* __restrict__ tile = bufs + parity * kN;
+        double2 v[kE];
+        {
+            const RegLayout& ly = slay[0];
+            uint32_t tp = 0;
+            for (uint32_t i = 0; i < kTB; ++i)
+                if ((threadIdx.x >> i) & 1u) tp |= 1u << ly.tpos[i];
+            const uint32_t p0 = 1u << ly.rpos[0], p1 = 1u << ly.rpos[1], p2 = 1u << ly.rpos[2],
+                           p3 = 1u << ly.rpos[3];
+#pragma unroll
+            for (int u = 0; u < kE; ++u)
+                v[u] = tile[tp | ((u & 1) ? p0 : 0) | ((u & 2) ? p1 : 0) | ((u & 4) ? p2 : 0) |
+                            ((u & 8) ? p3 : 0)];
+        }
+        __syncwarp();   // every lane's linear read before any lane's first remap write
+        uint32_t cur = 0;
+        for (uint32_t o = 0; o < p.n_ops; ++o) {
+            const RegOp& op = sops[o];
+            if ((base & op.gcmask) != op.gcmask) continue;
+            const uint32_t kind = op.kind;
+            if (kind == kRegRemap) {
+                {
+                    const RegLayout& ly = slay[cur];
+                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
+#pragma unroll
+                    for (int u = 0; u < kE; ++u)
+                        tile[ts ^ ((u & 1) ? r0 : 0) ^ ((u & 2) ? r1 : 0) ^ ((u & 4) ? r2 : 0) ^
+                             ((u & 8) ? r3 : 0)] = v[u];
+                }
+                cur = op.code;
+                const bool local = op.k != 0;
+                if (local) __syncwarp();
+                else __syncthreads();
+                {
+                    const RegLayout& ly = slay[cur];
+                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
+#pragma unroll
+                    for (int u = 0; u < kE; ++u)
+                        v[u] = tile[ts ^ ((u & 1) ? r0 : 0) ^ ((u & 2) ? r1 : 0) ^
+                                    ((u & 4) ? r2 : 0) ^ ((u & 8) ? r3 : 0)];
+                }
+                if (local) __syncwarp();
+                else __syncthreads();
+                continue;
+            }
+            const uint32_t tc = op.tcmask;
+            if ((threadIdx.x & tc) != tc) continue;
+            const uint32_t rc = op.rcmask;
+            uint32_t moff = op.mat_off;
+            if (const uint32_t nsel = op.nsel) {
+                uint32_t sel = 0;
+                for (uint32_t i = 0; i < nsel; ++i)
+                    sel |= static_cast<uint32_t>((base >> op.selq[i]) & 1u) << i;
+                const uint32_t k2 = kind == kRegDense ? 2u * op.k : op.k;
+                moff += sel << k2;
+            }
+            const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
+                                                     : smat_addr + 16u * moff;
+            if (kind == kRegDense) {
+                dispatch_dense(v, op.code, mat, rc);
+            } else if (kind == kRegPhase) {
+                const double2 f = lds2(mat);
+#pragma unroll
+                for (int u = 0; u < kE; ++u)
+                    if ((u & rc) == rc) v[u] = cmul(f, v[u]);
+            } else if (kind == kRegSwapX) {
+                dispatch_swapx(v, op.code, rc);
+            } else {
+                reg_diag(v, op, mat, rc);
+            }
+        }
+        {
+            const RegLayout& ly = slay[cur];
+            const uint64_t g = base | thread_goff(ly, kTB, stbit);
+            const uint64_t g0 = stbit[ly.rpos[0]], g1 = stbit[ly.rpos[1]], g2 = stbit[ly.rpos[2]],
+                           g3 = stbit[ly.rpos[3]];
+#pragma unroll
+            for (int u = 0; u < kE; ++u)
+                __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
+                            ((u & 8) ? g3 : 0)),
+                       v[u]);
+        }
+    }
+    cp_async_wait_all();
+}
+
+template <int M, int MINB>
+void launch_pipe(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
+                 const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
+    constexpr uint32_t kT = 1u << (M - kRegBits);
+    auto kern = k_regtile_pipe<M, MINB>;
+    cuda_check_launch_attr(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(kRegPipeMaxSmem)));
+    const uint32_t by_smem = static_cast<uint32_t>(std::max<size_t>(1, (227 * 1024) / (smem + 1024)));
+    const uint64_t want = static_cast<uint64_t>(ctx.num_sms) * std::min<uint32_t>(MINB, by_smem);
+    const uint32_t grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, p.n_tiles)));
+    kern<<<dim3(grid, batch), kT, smem, ctx.stream>>>(st, p, d_ops, d_layouts, d_mats);
+    check_launch("register tile pass (double-buffered)");
+}
+
 template <int M, int MINB>
 void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
                const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
@@ -501,11 +718,19 @@ void launch_m(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& 
 
 }  // namespace
 
-size_t reg_smem_bytes(const RegPass& pass) {
-    const size_t records = sizeof(double2) * ((size_t{1} << pass.m) + pass.n_mat) +
+size_t reg_smem_bytes(const RegPass& pass, uint32_t tiles) {
+    const size_t records = sizeof(double2) * ((size_t{tiles} << pass.m) + pass.n_mat) +
                            sizeof(RegOp) * pass.n_ops + sizeof(RegLayout) * pass.n_layouts;
     return pass.n_dyn ? ((records + 15) & ~size_t{15}) + sizeof(double2) * 2 * pass.dyn_entries
                       : records;
+}
+
+bool reg_pipe_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("LQCS_REG_PIPE");
+        return e != nullptr && std::atoi(e) != 0;
+    }();
+    return on;
 }
 
 void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
@@ -514,6 +739,16 @@ void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t bat
     RegPass p = pass;
     p.batch_stride = uint64_t{1} << n;
     p.n_tiles = (uint64_t{1} << n) >> p.m;
+    if (reg_pipe_enabled() && (p.m == 11 || p.m == 12)) {
+        const size_t smem2 = reg_smem_bytes(p, 2);
+        if (smem2 <= kRegPipeMaxSmem && p.n_ops <= kRegMaxRecords && p.n_mat <= kRegMaxMatrix &&
+            p.n_dyn <= kRegMaxDyn && p.dyn_entries <= kRegMaxDynEntries && p.n_layouts >= 1 &&
+            p.h <= kTileMaxHigh) {
+            if (p.m == 12) launch_pipe<12, 1>(ctx, st, batch, p, smem2, d_ops, d_layouts, d_mats);
+            else launch_pipe<11, 3>(ctx, st, batch, p, smem2, d_ops, d_layouts, d_mats);
+            return;
+        }
+    }
     const size_t smem = reg_smem_bytes(p);
     if (smem > kTileMaxSmem || p.m < kRegMinBits || p.m > kRegMaxBits || p.h > kTileMaxHigh ||
         p.n_layouts < 1 || p.n_ops > kRegMaxRecords || p.n_mat > kRegMaxMatrix ||

@@ -125,7 +125,8 @@ struct RegPass {
     uint32_t m, L, h;
     uint32_t n_ops, n_layouts, n_mat;
     uint32_t mat_stride;      // double2 between the matrices of consecutive states (0: shared)
-    uint32_t sync_tiles;      // some remap changes the warp bits: barrier between tiles
+    uint32_t sync_tiles;      // barrier between a CTA's tiles
+    uint32_t cta_remaps;      // some remap changes the warp bits (every warp's slot set)
     uint32_t hbits[kTileMaxHigh];
     uint32_t n_dyn;           // per-tile diagonals: their record indices and table entries
     uint32_t dyn_entries;
@@ -139,6 +140,8 @@ static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-b
 void launch_reg_pass(const LaunchCtx& ctx, double2* st, uint32_t n, uint32_t batch,
                      const RegPass& pass, const RegOp* d_ops, const RegLayout* d_layouts,
                      const double2* d_mats);
-size_t reg_smem_bytes(const RegPass& pass);
+// Shared memory of a register pass holding `tiles` tile buffers (2: double-buffered kernel).
+size_t reg_smem_bytes(const RegPass& pass, uint32_t tiles = 1);
+constexpr size_t kRegPipeMaxSmem = 220 * 1024;   // double-buffered kernel, one CTA per SM at m = 12
 
 }  // namespace lqcs_b200

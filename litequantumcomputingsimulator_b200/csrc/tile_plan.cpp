@@ -1217,8 +1217,8 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     // without it, the inverse QFT of 20 of 24 qubits (and Shor's circuit at 24 qubits)
     // came out wrong by ~1e-3, differently from run to run — some warp still used the
     // previous tile's shared memory while another started the next tile.
-    (void)sync_tiles;
     pass.sync_tiles = 1u;
+    pass.cta_remaps = sync_tiles ? 1u : 0u;
     for (uint32_t b = 0; b < m; ++b) {
         pass.store_qubit[b] = static_cast<uint8_t>(store_q[b]);
         const uint32_t home = b < cfg.L ? b : item.hbits[b - cfg.L];

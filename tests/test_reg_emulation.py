@@ -1,0 +1,123 @@
+"""Host emulation of the register tile kernel (lqcs_debug_emulate_register_passes): the
+records the planner lowers a circuit into are executed thread by thread on the CPU, as
+k_regtile and its double-buffered form execute them, and every shared-memory access is
+checked against the CUDA barrier model.  No GPU.
+
+* Values: brickwork, QFT, partial inverse QFT and random circuits of the gate types that
+  run inside register passes match the oracle within 1e-12, out of place, with every
+  amplitude stored exactly once by the tile that loaded it.
+* Races: none in the kernels as launched (barrier between tiles; double-buffered kernel),
+  none either with the barrier only in passes whose remaps change the warp bits (each warp
+  then keeps its own shared-memory slots from tile to tile), and many when that barrier is
+  dropped from passes that do change them — the check is sensitive.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import litequantumcomputingsimulator_b200 as lq
+from litequantumcomputingsimulator_b200 import _native as N
+from litequantumcomputingsimulator_b200 import workloads as W
+
+TOL = 1e-12
+BARRIER, NONE, PLANNED, PIPE = 1, 0, 2, 3
+
+
+def emulate(qc, mode, state=None, grid=296, race_ctas=4):
+    arr, cnt, _keep = qc.c_instructions()
+    passes, races = C.c_uint64(0), C.c_uint64(0)
+    report = C.create_string_buffer(512)
+    st = None if state is None else np.ascontiguousarray(np.array(state, dtype=np.complex128))
+    N.call("lqcs_debug_emulate_register_passes", qc.num_qubits(), arr, cnt, grid, mode,
+           st.ctypes.data if st is not None else None, race_ctas, C.byref(passes), C.byref(races),
+           report, 512)
+    return st, passes.value, races.value, report.value.decode()
+
+
+def tile_circuit(n, n_gates, seed):
+    rng = np.random.default_rng(seed)
+    qc = lq.QuantumCircuit(n)
+    for _ in range(n_gates):
+        a, b, c = (int(x) for x in rng.permutation(n)[:3])
+        ang = float(rng.uniform(-np.pi, np.pi))
+        k = int(rng.integers(12))
+        if k == 0:
+            qc.h(a)
+        elif k == 1:
+            qc.u(ang, 0.3 * ang, -ang, a)
+        elif k == 2:
+            qc.cx(a, b)
+        elif k == 3:
+            qc.cp(ang, a, b)
+        elif k == 4:
+            qc.rzz(ang, a, b)
+        elif k == 5:
+            qc.swap(a, b)
+        elif k == 6:
+            qc.ccx(a, b, c)
+        elif k == 7:
+            qc.mcp(ang, [a, b], c)
+        elif k == 8:
+            qc.t(a)
+        elif k == 9:
+            qc.crx(ang, a, b)
+        elif k == 10:
+            qc.iswap(a, b)
+        else:
+            qc.rxx(ang, a, b)
+    return qc
+
+
+def circuits():
+    yield "brickwork14", W.brickwork(14, 8, seed=3)
+    yield "brickwork17", W.brickwork(17, 6, seed=4)
+    q = lq.QuantumCircuit(16)
+    q.compose(lq.algorithms.qft_inverse(14))
+    yield "iqft16of14", q
+    yield "qft15", lq.algorithms.qft(15)
+    yield "random13", tile_circuit(13, 150, seed=5)
+    yield "random16", tile_circuit(16, 200, seed=6)
+
+
+@pytest.mark.parametrize("mode", [BARRIER, PIPE])
+@pytest.mark.parametrize("name,qc", list(circuits()), ids=[c[0] for c in circuits()])
+def test_emulated_passes_match_oracle(port, name, qc, mode):
+    n = qc.num_qubits()
+    init = W.gaussian_state(n, seed=n)
+    got, passes, races, report = emulate(qc, mode, init)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    assert passes >= 1
+    assert races == 0, report
+    assert np.max(np.abs(got - want)) < TOL
+
+
+@pytest.mark.parametrize("tile_bits", ["11", "12"])
+def test_double_buffered_tile_sizes(port, monkeypatch, tile_bits):
+    monkeypatch.setenv("LQCS_TILE_BITS", tile_bits)
+    qc = W.brickwork(15, 8, seed=9)
+    init = W.gaussian_state(15, seed=2)
+    got, _passes, races, report = emulate(qc, PIPE, init, grid=444)
+    assert races == 0, report
+    assert np.max(np.abs(got - port.run_statevector(qc, fuse=False, state=init))) < TOL
+
+
+@pytest.mark.parametrize("n,k", [(24, 20), (24, 16), (22, 19)])
+def test_partial_inverse_qft_barrier_model(n, k):
+    """The passes of the inverse QFT of k of n qubits (no remap changes the warp bits) are
+    race-free even without a barrier between tiles."""
+    qc = lq.QuantumCircuit(n)
+    qc.compose(lq.algorithms.qft_inverse(k))
+    for mode in (BARRIER, PLANNED, PIPE):
+        _st, _p, races, report = emulate(qc, mode, race_ctas=8)
+        assert races == 0, (mode, report)
+
+
+def test_race_check_is_sensitive():
+    """Passes whose CTA-wide remaps change the warp bits need the barrier between tiles:
+    without it the check must report races; with it (or as planned), none."""
+    qc = W.brickwork(22, 10, seed=2025)
+    _st, _p, races, report = emulate(qc, NONE, race_ctas=2)
+    assert races > 0 and "races with" in report
+    for mode in (PLANNED, BARRIER, PIPE):
+        assert emulate(qc, mode, race_ctas=2)[2] == 0
