@@ -470,15 +470,18 @@ uint64_t lqcs_kernel_launch_count(void);
  * with no counterpart in the reference).  Plans the circuit into register tile passes as
  * lqcs_program_create does with the tile-pass planner (the LQCS_TILE_* overrides apply)
  * and runs every pass thread by thread on the host: with `state` (2^n_qubits complex128,
- * interleaved, in/out) it computes the amplitudes, out of place, and fails if a pass writes
- * an amplitude other than exactly once; in any case it checks every shared-memory access
- * of the kernel against the barrier model (warps independent between CTA barriers, threads
- * of a warp independent between warp barriers) for a grid of `grid` CTAs (with state ==
- * NULL only the first `race_ctas` CTAs are walked).  sync_tiles: 1 = barrier between a
- * CTA's tiles (what the kernel runs), 0 = none, 2 = only in passes with a remap that changes
- * the warp bits, 3 = the double-buffered kernel (LQCS_REG_PIPE=1; 2^11- and 2^12-amplitude
- * tiles): asynchronous copies into two tile buffers and one barrier per tile.  *n_races counts racing accesses; `report` (capacity report_cap) receives
- * the first.  Fails if a gate does not run inside a register pass. */
+ * interleaved, in/out) it computes the amplitudes, out of place, fails if a pass stores an
+ * amplitude other than exactly once or one its tile did not load, and checks that no store
+ * can overtake another thread's load of the same amplitude (in place, a relabelling pass
+ * stores to places other warps load); in any case it checks every shared-memory access of
+ * the kernel against the barrier model (warps independent between CTA barriers, threads of
+ * a warp independent between warp barriers) for a grid of `grid` CTAs (with state == NULL
+ * only the first `race_ctas` CTAs are walked).  sync_tiles: 2 = as the kernel runs (a
+ * barrier between a CTA's tiles where a remap changes the warp bits), 1 = a barrier between
+ * all tiles, 0 = none, 3 = the double-buffered kernel (LQCS_REG_PIPE=1; 2^11- and
+ * 2^12-amplitude tiles); + 8 leaves out the barrier a relabelling pass puts between its
+ * loads and stores.  *n_races counts racing accesses; `report` (capacity report_cap)
+ * receives the first.  Fails if a gate does not run inside a register pass. */
 int lqcs_debug_emulate_register_passes(uint32_t n_qubits, const lqcs_instruction* insts,
                                        uint64_t n_insts, uint64_t grid, int32_t sync_tiles,
                                        double* state, uint64_t race_ctas, uint64_t* n_passes,

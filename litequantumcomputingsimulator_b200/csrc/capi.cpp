@@ -73,11 +73,12 @@ int lqcs_debug_emulate_register_passes(uint32_t n_qubits, const lqcs_instruction
         need(n_races, "n_races");
         if (n_qubits < lqcs_b200::kRegMinBits || n_qubits > 26)
             lqcs_b200::invalid("register tile emulation: n_qubits must be in [9, 26]");
-        if (sync_tiles < 0 || sync_tiles > 3)
-            lqcs_b200::invalid("register tile emulation: sync_tiles must be 0, 1, 2 or 3");
+        const int mode = sync_tiles & 7, drop = sync_tiles & 8;
+        if (mode > 3 || (sync_tiles & ~15))
+            lqcs_b200::invalid("register tile emulation: sync_tiles must be 0..3, optionally + 8");
         std::string first;
-        lqcs_b200::emulate_register_program(n_qubits, insts, n_insts, grid,
-                                            sync_tiles == 3 ? 1 : sync_tiles, sync_tiles == 3,
+        lqcs_b200::emulate_register_program(n_qubits, insts, n_insts, grid, mode == 3 ? 1 : mode,
+                                            mode == 3, drop != 0,
                                             reinterpret_cast<lqcs_b200::cd*>(state), race_ctas,
                                             n_passes, n_races, &first);
         if (report && report_cap) {

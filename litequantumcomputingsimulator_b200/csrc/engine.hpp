@@ -190,9 +190,9 @@ void sample(lqcs_state& st, const double* u, uint64_t shots, uint64_t* idx, doub
 // between tiles, 0 none, 2 where a remap changes the warp bits (RegPass::cta_remaps).
 // pipe: the double-buffered kernel's access pattern (tile sizes 2^11 and 2^12).
 void emulate_register_program(uint32_t n, const lqcs_instruction* insts, uint64_t n_insts,
-                              uint64_t grid, int sync_tiles, bool pipe, cd* state,
-                              uint64_t race_ctas, uint64_t* n_passes, uint64_t* n_races,
-                              std::string* report);
+                              uint64_t grid, int sync_tiles, bool pipe, bool drop_load_barrier,
+                              cd* state, uint64_t race_ctas, uint64_t* n_passes,
+                              uint64_t* n_races, std::string* report);
 
 uint32_t static_expectation_max_terms();
 void forget_static_scratch_addresses();   // after a device reset (lqcs_release_caches)

@@ -126,6 +126,16 @@ class CtaModel {
         }
     }
     uint32_t threads() const { return kT_; }
+    uint64_t epoch() const { return epoch_; }
+    uint64_t wepoch(uint32_t warp) const { return wepoch_[warp]; }
+    // Whether an access by `thread` now conflicts with an earlier one by (warp, wepoch,
+    // thread) in CTA-barrier interval `epoch` (the barrier model above, for global memory).
+    bool conflicts(uint64_t epoch, uint32_t warp, uint64_t wepoch, uint32_t other,
+                   uint32_t thread) const {
+        if (epoch != epoch_) return false;
+        if (warp != thread / 32) return true;
+        return wepoch == wepoch_[warp] && other != thread;
+    }
 
   private:
     uint32_t kT_, warps_;
@@ -174,6 +184,9 @@ uint64_t reg_goff(const RegLayout& ly, const uint64_t* gbit, uint32_t u) {
 struct AmpLog {
     std::vector<uint8_t> written;
     std::vector<uint64_t> owner;
+    // the load of each amplitude: CTA-barrier interval, warp, warp-barrier interval, thread
+    std::vector<uint64_t> ld_epoch, ld_wepoch;
+    std::vector<uint32_t> ld_thread;
 };
 
 // Emulate one register pass on `in` (read) / `out` (written; `amps` records stores and
@@ -185,11 +198,13 @@ struct AmpLog {
 // pipe: the double-buffered kernel (k_regtile_pipe) instead: each tile's amplitudes arrive
 // by asynchronous copies into one of two shared buffers (issued right after the previous
 // tile's barrier), are read linearly through layout 0, and the remaps use that buffer; its
-// per-tile tables are built before the tile's one barrier.
+// per-tile tables are built before the tile's one barrier.  drop_load_barrier: leave out the
+// barrier a relabelling pass puts between its loads and stores (to show that the in-place
+// check finds the hazard it prevents).
 void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* lays, const cd* mats,
                       uint32_t n, const cd* in, cd* out, AmpLog* amps,
                       uint64_t grid, uint64_t race_ctas, int sync_tiles, bool pipe,
-                      uint32_t pass_index, RaceLog& log) {
+                      bool drop_load_barrier, uint32_t pass_index, RaceLog& log) {
     RegPass p = pass;
     p.sync_tiles = sync_tiles == 2 ? p.cta_remaps : static_cast<uint32_t>(sync_tiles != 0);
     const uint32_t m = p.m;
@@ -231,7 +246,12 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                              pass_index);
                 if (in) {
                     smem[at] = in[a];
-                    if (amps) amps->owner[a] = tile;
+                    if (amps) {
+                        amps->owner[a] = tile;
+                        amps->ld_epoch[a] = model.epoch();
+                        amps->ld_wepoch[a] = model.wepoch(model.async_thread() / 32);
+                        amps->ld_thread[a] = model.async_thread();
+                    }
                 }
             }
         }
@@ -253,10 +273,16 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                     for (uint32_t u = 0; u < kE; ++u) {
                         const uint64_t a = g | reg_goff(ly, gbit, u);
                         v[t * kE + u] = in[a];
-                        if (amps) amps->owner[a] = tid;
+                        if (amps) {
+                            amps->owner[a] = tid;
+                            amps->ld_epoch[a] = model.epoch();
+                            amps->ld_wepoch[a] = model.wepoch(t / 32);
+                            amps->ld_thread[a] = t;
+                        }
                     }
                 }
             }
+            if (!pipe && p.load_barrier && !drop_load_barrier) model.cta_barrier();
             // per-tile diagonal tables
             const uint32_t dyn_base = parity * p.dyn_entries;
             if (p.n_dyn) {
@@ -426,6 +452,21 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                         out[a] = v[t * kE + u];
                         if (amps) {
                             ++amps->written[a];
+                            // in place: a store may not overtake another thread's load of
+                            // the same amplitude (a pass that relabels stores to places
+                            // other warps load)
+                            if (model.conflicts(amps->ld_epoch[a], amps->ld_thread[a] / 32,
+                                                amps->ld_wepoch[a], amps->ld_thread[a], t)) {
+                                if (log.races == 0) {
+                                    std::ostringstream os;
+                                    os << "pass " << pass_index << ", tile " << tid
+                                       << ": store of amplitude " << a << " by thread " << t
+                                       << " may overtake its load by thread " << amps->ld_thread[a]
+                                       << " (no barrier between them)";
+                                    log.first = os.str();
+                                }
+                                ++log.races;
+                            }
                             if (amps->owner[a] != tid)
                                 logic("register tile emulation: pass " + std::to_string(pass_index) +
                                       ", tile " + std::to_string(tid) + " stores amplitude " +
@@ -442,9 +483,9 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
 // Plan and lower a circuit into register tile passes with the default tile configuration
 // (environment overrides included) and emulate every pass; see lqcs_debug_emulate_register_passes.
 void emulate_register_program(uint32_t n, const lqcs_instruction* insts, uint64_t n_insts,
-                              uint64_t grid, int sync_tiles, bool pipe, cd* state,
-                              uint64_t race_ctas, uint64_t* n_passes, uint64_t* n_races,
-                              std::string* report) {
+                              uint64_t grid, int sync_tiles, bool pipe, bool drop_load_barrier,
+                              cd* state, uint64_t race_ctas, uint64_t* n_passes,
+                              uint64_t* n_races, std::string* report) {
     const auto gates = decode_all(insts, n_insts, n);
     const TileConfig cfg = default_tile_config(n);
     if (!cfg.reg) invalid("register tile emulation: register passes are switched off");
@@ -456,6 +497,9 @@ void emulate_register_program(uint32_t n, const lqcs_instruction* insts, uint64_
     if (state) {
         next.resize(size_t{1} << n);
         amps.owner.resize(size_t{1} << n);
+        amps.ld_epoch.resize(size_t{1} << n);
+        amps.ld_wepoch.resize(size_t{1} << n);
+        amps.ld_thread.resize(size_t{1} << n);
     }
     for (const PlanItem& it : items) {
         if (!it.is_pass)
@@ -472,7 +516,8 @@ void emulate_register_program(uint32_t n, const lqcs_instruction* insts, uint64_
         if (state) amps.written.assign(size_t{1} << n, 0);
         emulate_reg_pass(rp, ops.data(), lays.data(), mats.data(), n, state, state ? next.data() : nullptr,
                          state ? &amps : nullptr, grid, race_ctas, sync_tiles,
-                         pipe && (rp.m == 11 || rp.m == 12), static_cast<uint32_t>(passes), log);
+                         pipe && (rp.m == 11 || rp.m == 12), drop_load_barrier,
+                         static_cast<uint32_t>(passes), log);
         if (state) {
             for (size_t a = 0; a < amps.written.size(); ++a)
                 if (amps.written[a] != 1)

@@ -351,6 +351,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                 v[u] = __ldcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
                                    ((u & 8) ? g3 : 0)));
         }
+        // relabelled stores go to places other warps load: all loads before any store
+        if (p.load_barrier) __syncthreads();
         // Start the HBM reads of this CTA's next tile into L2 while this one computes, so
         // its loads above hit L2 on the next iteration.  Thread r < 2^h takes the row of
         // high-bit pattern r: 2^L contiguous amplitudes, 16 B * 2^L from a 16 B boundary.

@@ -133,6 +133,8 @@ struct RegPass {
     uint8_t dyn_rec[kRegMaxDyn];
     uint32_t relabel;         // SWAPs relabelled tile bits: tile bit b is stored to the place
     uint8_t store_qubit[kRegMaxBits];   // of qubit store_qubit[b]
+    uint32_t load_barrier;    // a barrier between the tile's loads and stores is needed and no
+                              // other barrier provides it (relabelled stores, in place)
 };
 
 static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");

@@ -1213,12 +1213,14 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     pass.n_layouts = static_cast<uint32_t>(lays.size());
     pass.n_mat = static_cast<uint32_t>(n_mat);
     pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
-    // A barrier between tiles in every pass, not only where a remap changed the warp bits:
-    // without it, the inverse QFT of 20 of 24 qubits (and Shor's circuit at 24 qubits)
-    // came out wrong by ~1e-3, differently from run to run — some warp still used the
-    // previous tile's shared memory while another started the next tile.
-    pass.sync_tiles = 1u;
-    pass.cta_remaps = sync_tiles ? 1u : 0u;
+    // A barrier between a CTA's tiles only where some remap changes the warp bits: then a
+    // warp's shared-memory slots in the last layout of one tile are not its slots in the first
+    // layout of the next.  Where every remap keeps them, each warp only ever touches its own
+    // slots (tile_swizzle is linear and the warp bits are the same high tile bits in every
+    // layout), so no warp can overtake another into shared memory that one still uses; the
+    // host emulation (reg_emulate.cpp) checks this against the barrier model.
+    pass.sync_tiles = sync_tiles ? 1u : 0u;
+    pass.cta_remaps = pass.sync_tiles;
     for (uint32_t b = 0; b < m; ++b) {
         pass.store_qubit[b] = static_cast<uint8_t>(store_q[b]);
         const uint32_t home = b < cfg.L ? b : item.hbits[b - cfg.L];
@@ -1226,6 +1228,11 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     }
     pass.n_dyn = static_cast<uint32_t>(dyn_rec.size());
     pass.dyn_entries = dyn_entries;
+    // A relabelling pass stores amplitudes, in place, to places that other threads (of other
+    // warps) load: every load of the tile must come before any store.  A CTA-wide remap or
+    // the per-tile table barrier, both after the loads, order them; otherwise the kernel
+    // adds a barrier after the loads.
+    pass.load_barrier = pass.relabel && !sync_tiles && dyn_rec.empty() ? 1u : 0u;
     for (size_t d = 0; d < dyn_rec.size(); ++d) pass.dyn_rec[d] = static_cast<uint8_t>(dyn_rec[d]);
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());
     layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());

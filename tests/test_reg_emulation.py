@@ -6,10 +6,15 @@ checked against the CUDA barrier model.  No GPU.
 * Values: brickwork, QFT, partial inverse QFT and random circuits of the gate types that
   run inside register passes match the oracle within 1e-12, out of place, with every
   amplitude stored exactly once by the tile that loaded it.
-* Races: none in the kernels as launched (barrier between tiles; double-buffered kernel),
-  none either with the barrier only in passes whose remaps change the warp bits (each warp
-  then keeps its own shared-memory slots from tile to tile), and many when that barrier is
-  dropped from passes that do change them — the check is sensitive.
+* Races: none in the kernels as launched (a barrier between tiles only in passes whose
+  remaps change the warp bits — elsewhere each warp keeps its own shared-memory slots from
+  tile to tile; the double-buffered kernel), and many when that barrier is dropped from
+  passes that do change them — the check is sensitive.
+* In place: a pass that relabels tile bits (SWAPs of two tile qubits) stores amplitudes to
+  places other warps load.  Without a barrier between the tile's loads and its stores a fast
+  warp can overwrite an amplitude before a slow warp has read it; this made QFT(n >= 24)
+  wrong by ~1e-4..1e-3 on the device when two CTAs shared an SM.  The kernel adds that
+  barrier where no remap or table barrier provides it; the check finds the hazard without it.
 """
 import ctypes as C
 
@@ -21,7 +26,8 @@ from litequantumcomputingsimulator_b200 import _native as N
 from litequantumcomputingsimulator_b200 import workloads as W
 
 TOL = 1e-12
-BARRIER, NONE, PLANNED, PIPE = 1, 0, 2, 3
+BARRIER, NONE, PLANNED, PIPE = 1, 0, 2, 3   # PLANNED: the barriers k_regtile runs with
+NO_LOAD_BARRIER = 8
 
 
 def emulate(qc, mode, state=None, grid=296, race_ctas=4):
@@ -80,7 +86,7 @@ def circuits():
     yield "random16", tile_circuit(16, 200, seed=6)
 
 
-@pytest.mark.parametrize("mode", [BARRIER, PIPE])
+@pytest.mark.parametrize("mode", [PLANNED, BARRIER, PIPE])
 @pytest.mark.parametrize("name,qc", list(circuits()), ids=[c[0] for c in circuits()])
 def test_emulated_passes_match_oracle(port, name, qc, mode):
     n = qc.num_qubits()
@@ -121,3 +127,18 @@ def test_race_check_is_sensitive():
     assert races > 0 and "races with" in report
     for mode in (PLANNED, BARRIER, PIPE):
         assert emulate(qc, mode, race_ctas=2)[2] == 0
+
+
+@pytest.mark.parametrize("n", [18, 20])
+def test_relabelled_store_needs_the_load_barrier(port, n):
+    """QFT(n) ends with qubit-reversal SWAPs, relabelled in its last pass: with the pass's
+    load barrier no store can overtake another thread's load; without it the check reports
+    the hazard (values of the out-of-place emulation are right either way)."""
+    qc = lq.algorithms.qft(n)
+    init = W.gaussian_state(n, seed=n + 3)
+    want = port.run_statevector(qc, fuse=False, state=init)
+    got, _p, races, report = emulate(qc, PLANNED, init)
+    assert races == 0, report
+    assert np.max(np.abs(got - want)) < TOL
+    _got, _p, races, report = emulate(qc, PLANNED + NO_LOAD_BARRIER, init)
+    assert races > 0 and "may overtake its load" in report
