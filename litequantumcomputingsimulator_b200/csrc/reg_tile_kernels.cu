@@ -58,19 +58,26 @@ __device__ __forceinline__ double2 lds2(uint32_t saddr) {
     return r;
 }
 
+// Matrix entries of an operation, entry i at 16 * i bytes of shared memory (the helpers
+// below take any functor of this shape).
+struct SharedMat {
+    uint32_t base;   // shared-memory address
+    __device__ __forceinline__ double2 operator()(uint32_t i) const { return lds2(base + 16u * i); }
+};
+
 // Group base of the g-th group of a target mask: g spread over the bits outside TM.
 __host__ __device__ constexpr int group_base(int g, int tm) { return deposit4(g, (kE - 1) & ~tm); }
 
 // Dense operation without register controls: one basic block, so the compiler interleaves
 // the groups.  Two-target operations take two groups per matrix read (each entry is loaded
 // twice per operation instead of four times).
-template <int TM>
-__device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
+template <int TM, class MS>
+__device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], const MS& mat) {
     constexpr int K = popc4(TM);
     constexpr int D = 1 << K;
     constexpr int G = kE / D;   // groups
     if constexpr (K == 1) {
-        const double2 m0 = lds2(mat), m1 = lds2(mat + 16), m2 = lds2(mat + 32), m3 = lds2(mat + 48);
+        const double2 m0 = mat(0), m1 = mat(1), m2 = mat(2), m3 = mat(3);
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             const int b = group_base(g, TM);
@@ -85,7 +92,7 @@ __device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
             double2 y0[D], y1[D];
 #pragma unroll
             for (int r = 0; r < D; ++r) {
-                const double2 mr = lds2(mat + 16u * (r * D));
+                const double2 mr = mat(r * D);
                 y0[r] = cmul(mr, v[b0]);
                 y1[r] = cmul(mr, v[b1]);
             }
@@ -93,7 +100,7 @@ __device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
             for (int c = 1; c < D; ++c) {
 #pragma unroll
                 for (int r = 0; r < D; ++r) {
-                    const double2 mr = lds2(mat + 16u * (r * D + c));
+                    const double2 mr = mat(r * D + c);
                     y0[r] = cmad(mr, v[b0 | deposit4(c, TM)], y0[r]);
                     y1[r] = cmad(mr, v[b1 | deposit4(c, TM)], y1[r]);
                 }
@@ -111,10 +118,10 @@ __device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
             double2 y[D];
 #pragma unroll
             for (int r = 0; r < D; ++r) {
-                double2 acc = cmul(lds2(mat + 16u * (r * D)), v[b]);
+                double2 acc = cmul(mat(r * D), v[b]);
 #pragma unroll
                 for (int c = 1; c < D; ++c)
-                    acc = cmad(lds2(mat + 16u * (r * D + c)), v[b | deposit4(c, TM)], acc);
+                    acc = cmad(mat(r * D + c), v[b | deposit4(c, TM)], acc);
                 y[r] = acc;
             }
 #pragma unroll
@@ -124,12 +131,12 @@ __device__ __forceinline__ void reg_dense_free(double2 (&v)[kE], uint32_t mat) {
 }
 
 // Dense operation with register controls: groups whose control bits are not all 1 skip.
-template <int TM>
-__device__ __forceinline__ void reg_dense(double2 (&v)[kE], uint32_t mat, uint32_t rcmask) {
+template <int TM, class MS>
+__device__ __forceinline__ void reg_dense(double2 (&v)[kE], const MS& mat, uint32_t rcmask) {
     constexpr int K = popc4(TM);
     constexpr int D = 1 << K;
     if constexpr (K == 1) {
-        const double2 m0 = lds2(mat), m1 = lds2(mat + 16), m2 = lds2(mat + 32), m3 = lds2(mat + 48);
+        const double2 m0 = mat(0), m1 = mat(1), m2 = mat(2), m3 = mat(3);
 #pragma unroll
         for (int b = 0; b < kE; ++b) {
             if (b & TM) continue;
@@ -146,10 +153,10 @@ __device__ __forceinline__ void reg_dense(double2 (&v)[kE], uint32_t mat, uint32
             double2 y[D];
 #pragma unroll
             for (int r = 0; r < D; ++r) {
-                double2 acc = cmul(lds2(mat + 16u * (r * D)), v[b | deposit4(0, TM)]);
+                double2 acc = cmul(mat(r * D), v[b | deposit4(0, TM)]);
 #pragma unroll
                 for (int c = 1; c < D; ++c)
-                    acc = cmad(lds2(mat + 16u * (r * D + c)), v[b | deposit4(c, TM)], acc);
+                    acc = cmad(mat(r * D + c), v[b | deposit4(c, TM)], acc);
                 y[r] = acc;
             }
 #pragma unroll
@@ -170,7 +177,8 @@ __device__ __forceinline__ void reg_swapx(double2 (&v)[kE], uint32_t rcmask) {
     }
 }
 
-__device__ __forceinline__ void dispatch_dense(double2 (&v)[kE], uint32_t code, uint32_t mat,
+template <class MS>
+__device__ __forceinline__ void dispatch_dense(double2 (&v)[kE], uint32_t code, const MS& mat,
                                                uint32_t rcmask) {
     if (rcmask == 0) {
         switch (code) {
@@ -223,8 +231,8 @@ __device__ __forceinline__ void dispatch_swapx(double2 (&v)[kE], uint32_t code, 
 // Diagonal whose entry bits sit on register-index bits R (and on thread bits, fixed per
 // thread in tpart): amplitude u takes entry tpart | e(u & R), so a thread loads each of its
 // 2^|R| distinct entries once and multiplies the 16 / 2^|R| amplitudes that share it.
-template <int R>
-__device__ __forceinline__ void reg_diag_r(double2 (&v)[kE], uint32_t mat, uint32_t rcmask,
+template <int R, class MS>
+__device__ __forceinline__ void reg_diag_r(double2 (&v)[kE], const MS& mat, uint32_t rcmask,
                                            uint32_t tpart, uint32_t rb0, uint32_t rb1,
                                            uint32_t rb2, uint32_t rb3) {
 #pragma unroll
@@ -232,7 +240,7 @@ __device__ __forceinline__ void reg_diag_r(double2 (&v)[kE], uint32_t mat, uint3
         if ((pt & R) != pt) continue;
         const uint32_t e = tpart | ((pt & 1) ? rb0 : 0u) | ((pt & 2) ? rb1 : 0u) |
                            ((pt & 4) ? rb2 : 0u) | ((pt & 8) ? rb3 : 0u);
-        const double2 f = lds2(mat + 16u * e);
+        const double2 f = mat(e);
 #pragma unroll
         for (int u = 0; u < kE; ++u)
             if ((u & R) == pt && (u & rcmask) == rcmask) v[u] = cmul(f, v[u]);
@@ -240,7 +248,8 @@ __device__ __forceinline__ void reg_diag_r(double2 (&v)[kE], uint32_t mat, uint3
 }
 
 // Entry (tpart | bits picked from u) of a diagonal for every amplitude u.
-__device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, uint32_t mat,
+template <class MS>
+__device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, const MS& mat,
                                          uint32_t rcmask) {
     uint32_t tpart = 0, rb0 = 0, rb1 = 0, rb2 = 0, rb3 = 0;   // entry bit of register bit i
     const uint32_t k = op.k;
@@ -436,7 +445,7 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
                                                      : smat_addr + 16u * moff;
             if (kind == kRegDense) {
-                dispatch_dense(v, op.code, mat, rc);
+                dispatch_dense(v, op.code, SharedMat{mat}, rc);
             } else if (kind == kRegPhase) {
                 const double2 f = lds2(mat);
 #pragma unroll
@@ -445,7 +454,7 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             } else if (kind == kRegSwapX) {
                 dispatch_swapx(v, op.code, rc);
             } else {
-                reg_diag(v, op, mat, rc);
+                reg_diag(v, op, SharedMat{mat}, rc);
             }
         }
         {
@@ -638,7 +647,7 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
             const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
                                                      : smat_addr + 16u * moff;
             if (kind == kRegDense) {
-                dispatch_dense(v, op.code, mat, rc);
+                dispatch_dense(v, op.code, SharedMat{mat}, rc);
             } else if (kind == kRegPhase) {
                 const double2 f = lds2(mat);
 #pragma unroll
@@ -647,7 +656,7 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
             } else if (kind == kRegSwapX) {
                 dispatch_swapx(v, op.code, rc);
             } else {
-                reg_diag(v, op, mat, rc);
+                reg_diag(v, op, SharedMat{mat}, rc);
             }
         }
         {
@@ -712,6 +721,17 @@ void launch_m(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& 
         launch_mb<12, 1>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
     } else if constexpr (M == 13) {
         launch_mb<13, 1>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    } else if constexpr (M == 11) {
+        // three 168-register CTAs per SM by default; LQCS_TILE_OCC=4: four of 128 registers
+        static const int occ = [] {
+            const char* e = std::getenv("LQCS_TILE_OCC");
+            return e ? std::atoi(e) : 3;
+        }();
+        if (occ >= 4) {
+            launch_mb<11, 4>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+            return;
+        }
+        launch_mb<11, 3>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
     } else {
         constexpr int kMinB = 65536 / ((1 << (M - kRegBits)) * 168);
         launch_mb<M, kMinB>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
