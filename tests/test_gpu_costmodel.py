@@ -1,6 +1,7 @@
 """The learned cost model: its FP32 GPU gradient against an FP64 CPU oracle of the same
-network, training, and what the trained model gains over the greedy plan (measured device
-time, identical amplitudes)."""
+network, training, and how well the trained model alone ranks the candidate plans of a
+held-out circuit (measured device time of its pick against every candidate's, identical
+amplitudes)."""
 import numpy as np
 import pytest
 import torch
@@ -82,7 +83,23 @@ def _time_ms(prog, sv, reps=5):
     return float(np.median(times))
 
 
-def test_learned_plan_versus_greedy():
+def _candidate_times(circuit, init):
+    """Measured device time of every candidate plan the learned mode chooses among."""
+    out = {}
+    for name, prog in CM.candidate_programs(circuit):
+        sv = lq.Statevector.from_numpy(init)
+        out[name] = _time_ms(prog, sv, reps=3)
+    return out
+
+
+def test_learned_plan_ranking(monkeypatch):
+    """Trained on the engine's own timings of five random-mix circuits, the model alone
+    (LQCS_LEARNED_JUDGE=1: no candidate is timed) must pick, for a held-out circuit, a plan
+    within 15 % of the fastest candidate and faster than the greedy plan, with amplitudes
+    equal to the greedy plan's.  It is not required to beat the default plan (register tile
+    passes of 2^12 amplitudes): on these circuits the default is the fastest candidate or
+    within a few percent of it, so the model's value is choosing without timing candidates
+    (what the autotuner does), not a faster plan than the default."""
     train_set = [W.random_mix_circuit(n, d, seed) for n, d, seed in
                  [(19, 12, 1), (20, 16, 2), (21, 10, 3), (20, 20, 4), (21, 14, 5)]]
     x, y = CM.collect(train_set)
@@ -90,6 +107,7 @@ def test_learned_plan_versus_greedy():
     assert loss < 0.5 * float(np.var(y))
     held = W.random_mix_circuit(21, 24, seed=99)
     init = W.gaussian_state(21, seed=7)
+    monkeypatch.setenv("LQCS_LEARNED_JUDGE", "1")
     greedy = lq.simulator.CompiledCircuit(held, True, 0, CM.GREEDY)
     learned = lq.simulator.CompiledCircuit(held, True, 0, CM.LEARNED)
     outs = []
@@ -98,12 +116,13 @@ def test_learned_plan_versus_greedy():
         prog.apply(sv)
         outs.append(sv.to_numpy())
     assert np.max(np.abs(outs[0] - outs[1])) < 1e-12
+    times = _candidate_times(held, init)
     sv = lq.Statevector.from_numpy(init)
-    t_greedy = _time_ms(greedy, sv)
     t_learned = _time_ms(learned, sv)
-    # the model picks among plans that include the greedy one; it must not lose more than
-    # the noise of the measurement
-    assert t_learned <= 1.10 * t_greedy, (t_learned, t_greedy)
+    t_greedy = _time_ms(greedy, sv)
+    best = min(times.values())
+    assert t_learned <= 1.15 * best, (t_learned, times)
+    assert t_learned < t_greedy, (t_learned, t_greedy)
     CM.clear()
     fallback = lq.simulator.CompiledCircuit(held, True, 0, CM.LEARNED)
     assert fallback.n_ops == greedy.n_ops
