@@ -24,6 +24,7 @@ namespace lqcs_b200 {
 namespace {
 
 constexpr int kE = 1 << kRegBits;   // amplitudes per thread
+constexpr uint32_t kRegSlotLayouts = 16;   // layouts whose per-thread slots are tabulated
 
 void check_launch(const char* what) {
     const cudaError_t e = cudaGetLastError();
@@ -311,6 +312,13 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
     __shared__ uint64_t sgbit[kRegMaxBits];   // and at the store (relabelled by SWAPs)
     __shared__ uint32_t shbits[kTileMaxHigh];
     __shared__ uint32_t sdynrec[kRegMaxDyn];
+    // per-thread constants of every tile, computed once: the global offsets of the thread
+    // bits at the load (layout 0) and at the store (the last layout), and each layout's
+    // shared-memory slot of the thread (the first kRegSlotLayouts layouts); the register
+    // bits' offsets are the same for every thread
+    __shared__ uint64_t s_ldg[kT], s_stg[kT];
+    __shared__ uint64_t s_ldr[kRegBits], s_str[kRegBits];
+    __shared__ uint16_t s_tslot[kRegSlotLayouts * kT];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (uint32_t i = 0; i < kTileMaxHigh; ++i) shbits[i] = p.hbits[i];   // static indices
@@ -339,6 +347,21 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             dst[w] = src[w];
     }
     __syncthreads();
+    {
+        uint32_t last = 0;   // remaps are never skipped: the store layout is the last one's
+        for (uint32_t o = 0; o < p.n_ops; ++o)
+            if (sops[o].kind == kRegRemap) last = sops[o].code;
+        s_ldg[threadIdx.x] = thread_goff(slay[0], kTB, gbit);
+        s_stg[threadIdx.x] = thread_goff(slay[last], kTB, stbit);
+        for (uint32_t l = 0; l < p.n_layouts && l < kRegSlotLayouts; ++l)
+            s_tslot[l * kT + threadIdx.x] = static_cast<uint16_t>(thread_slot(slay[l], kTB));
+        if (threadIdx.x < kRegBits) {
+            s_ldr[threadIdx.x] = gbit[slay[0].rpos[threadIdx.x]];
+            s_str[threadIdx.x] = stbit[slay[last].rpos[threadIdx.x]];
+        }
+    }
+    __syncthreads();
+    const bool slot_table = p.n_layouts <= kRegSlotLayouts;   // uniform
     const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
     const uint32_t sdyn_addr = static_cast<uint32_t>(__cvta_generic_to_shared(sdyn));
     double2* __restrict__ s = st + static_cast<uint64_t>(blockIdx.y) * p.batch_stride;
@@ -351,10 +374,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
         for (uint32_t i = 0; i < p.h; ++i) base = insert_zero_bit(base, shbits[i]);
         double2 v[kE];
         {
-            const RegLayout& ly = slay[0];
-            const uint64_t g = base | thread_goff(ly, kTB, gbit);
-            const uint64_t g0 = gbit[ly.rpos[0]], g1 = gbit[ly.rpos[1]], g2 = gbit[ly.rpos[2]],
-                           g3 = gbit[ly.rpos[3]];
+            const uint64_t g = base | s_ldg[threadIdx.x];
+            const uint64_t g0 = s_ldr[0], g1 = s_ldr[1], g2 = s_ldr[2], g3 = s_ldr[3];
 #pragma unroll
             for (int u = 0; u < kE; ++u)
                 v[u] = __ldcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
@@ -407,7 +428,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             if (kind == kRegRemap) {
                 {
                     const RegLayout& ly = slay[cur];
-                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t ts = slot_table ? s_tslot[cur * kT + threadIdx.x]
+                                                   : thread_slot(ly, kTB);
                     const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
 #pragma unroll
                     for (int u = 0; u < kE; ++u)
@@ -420,7 +442,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                 else __syncthreads();
                 {
                     const RegLayout& ly = slay[cur];
-                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t ts = slot_table ? s_tslot[cur * kT + threadIdx.x]
+                                                   : thread_slot(ly, kTB);
                     const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
 #pragma unroll
                     for (int u = 0; u < kE; ++u)
@@ -458,10 +481,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
             }
         }
         {
-            const RegLayout& ly = slay[cur];
-            const uint64_t g = base | thread_goff(ly, kTB, stbit);
-            const uint64_t g0 = stbit[ly.rpos[0]], g1 = stbit[ly.rpos[1]], g2 = stbit[ly.rpos[2]],
-                           g3 = stbit[ly.rpos[3]];
+            const uint64_t g = base | s_stg[threadIdx.x];
+            const uint64_t g0 = s_str[0], g1 = s_str[1], g2 = s_str[2], g3 = s_str[3];
 #pragma unroll
             for (int u = 0; u < kE; ++u)
                 __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
@@ -507,6 +528,13 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
     __shared__ uint64_t sgbit[kRegMaxBits];
     __shared__ uint32_t shbits[kTileMaxHigh];
     __shared__ uint32_t sdynrec[kRegMaxDyn];
+    // per-thread constants of every tile, computed once: the global offsets of the thread
+    // bits at the load (layout 0) and at the store (the last layout), and each layout's
+    // shared-memory slot of the thread (the first kRegSlotLayouts layouts); the register
+    // bits' offsets are the same for every thread
+    __shared__ uint64_t s_ldg[kT], s_stg[kT];
+    __shared__ uint64_t s_ldr[kRegBits], s_str[kRegBits];
+    __shared__ uint16_t s_tslot[kRegSlotLayouts * kT];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (uint32_t i = 0; i < kTileMaxHigh; ++i) shbits[i] = p.hbits[i];
@@ -535,6 +563,21 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
             dst[w] = src[w];
     }
     __syncthreads();
+    {
+        uint32_t last = 0;   // remaps are never skipped: the store layout is the last one's
+        for (uint32_t o = 0; o < p.n_ops; ++o)
+            if (sops[o].kind == kRegRemap) last = sops[o].code;
+        s_ldg[threadIdx.x] = thread_goff(slay[0], kTB, gbit);
+        s_stg[threadIdx.x] = thread_goff(slay[last], kTB, stbit);
+        for (uint32_t l = 0; l < p.n_layouts && l < kRegSlotLayouts; ++l)
+            s_tslot[l * kT + threadIdx.x] = static_cast<uint16_t>(thread_slot(slay[l], kTB));
+        if (threadIdx.x < kRegBits) {
+            s_ldr[threadIdx.x] = gbit[slay[0].rpos[threadIdx.x]];
+            s_str[threadIdx.x] = stbit[slay[last].rpos[threadIdx.x]];
+        }
+    }
+    __syncthreads();
+    const bool slot_table = p.n_layouts <= kRegSlotLayouts;   // uniform
     const uint32_t smat_addr = static_cast<uint32_t>(__cvta_generic_to_shared(smat));
     const uint32_t sdyn_addr = static_cast<uint32_t>(__cvta_generic_to_shared(sdyn));
     const uint32_t bufs_addr = static_cast<uint32_t>(__cvta_generic_to_shared(bufs));
@@ -609,7 +652,8 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
             if (kind == kRegRemap) {
                 {
                     const RegLayout& ly = slay[cur];
-                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t ts = slot_table ? s_tslot[cur * kT + threadIdx.x]
+                                                   : thread_slot(ly, kTB);
                     const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
 #pragma unroll
                     for (int u = 0; u < kE; ++u)
@@ -622,7 +666,8 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
                 else __syncthreads();
                 {
                     const RegLayout& ly = slay[cur];
-                    const uint32_t ts = thread_slot(ly, kTB);
+                    const uint32_t ts = slot_table ? s_tslot[cur * kT + threadIdx.x]
+                                                   : thread_slot(ly, kTB);
                     const uint32_t r0 = ly.rsw[0], r1 = ly.rsw[1], r2 = ly.rsw[2], r3 = ly.rsw[3];
 #pragma unroll
                     for (int u = 0; u < kE; ++u)
@@ -660,10 +705,8 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
             }
         }
         {
-            const RegLayout& ly = slay[cur];
-            const uint64_t g = base | thread_goff(ly, kTB, stbit);
-            const uint64_t g0 = stbit[ly.rpos[0]], g1 = stbit[ly.rpos[1]], g2 = stbit[ly.rpos[2]],
-                           g3 = stbit[ly.rpos[3]];
+            const uint64_t g = base | s_stg[threadIdx.x];
+            const uint64_t g0 = s_str[0], g1 = s_str[1], g2 = s_str[2], g3 = s_str[3];
 #pragma unroll
             for (int u = 0; u < kE; ++u)
                 __stcs(s + (g | ((u & 1) ? g0 : 0) | ((u & 2) ? g1 : 0) | ((u & 4) ? g2 : 0) |
@@ -695,7 +738,13 @@ void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass&
     auto kern = k_regtile<M, MINB>;
     cuda_check_launch_attr(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kTileMaxSmem)));
-    const uint32_t by_smem = static_cast<uint32_t>(std::max<size_t>(1, (227 * 1024) / (smem + 1024)));
+    static const size_t static_smem = [&] {
+        cudaFuncAttributes a{};
+        cuda_check_launch_attr(cudaFuncGetAttributes(&a, kern));
+        return a.sharedSizeBytes;
+    }();
+    const uint32_t by_smem = static_cast<uint32_t>(
+        std::max<size_t>(1, (227 * 1024) / (smem + static_smem + 1024)));
     const uint64_t want = static_cast<uint64_t>(ctx.num_sms) * std::min<uint32_t>(MINB, by_smem);
     const uint32_t grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, p.n_tiles)));
     kern<<<dim3(grid, batch), kT, smem, ctx.stream>>>(st, p, d_ops, d_layouts, d_mats);
