@@ -5,11 +5,12 @@ gradient workload.
   Gaussian state, through the default path (register tile passes with searched high
   qubits), against the engine's own gate-by-gate path on a second 16 GiB state; compared on
   the device in chunks.
-* 28 and 30 qubits against the reference compiled from its own sources: the first two
-  brickwork layers of the headline circuit (from |0..0>, `StatevectorSimulator::
-  run_statevector`, src/backend/statevector_simulator.cpp:222-230) and QFT(28) on a Gaussian
-  state (src/algorithms/qft.cpp:7-23, applied by the reference's kernels).  The 30-qubit
-  case holds three 16 GiB host arrays and runs only where the host has the memory.
+* 26 to 30 qubits against the reference compiled from its own sources: the first two
+  brickwork layers of the headline circuit at 28 and 30 qubits (from |0..0>,
+  `StatevectorSimulator::run_statevector`, src/backend/statevector_simulator.cpp:222-230)
+  and QFT(26) on a Gaussian state (src/algorithms/qft.cpp:7-23, applied by the reference's
+  kernels); QFT(28) against the DFT it computes.  The 30-qubit case holds three 16 GiB
+  host arrays and runs only where the host has the memory.
 * 16 qubits, 200 Pauli rotations of weight 2..8, 500 Hamiltonian terms, 256 parameter sets
   in one batched adjoint call: sets 0 and 255 against the reference's parameter-shift
   gradient (src/algorithms/vqe.cpp:68-94) within 1e-9, energies within 1e-11, and ten
@@ -121,12 +122,25 @@ def test_brickwork_30q_two_layers_vs_reference(threads):
     assert _host_maxdiff(got, want) < TOL
 
 
-def test_qft28_on_gaussian_state_vs_reference(threads):
-    init = W.gaussian_state(28, seed=28)
-    q = lq.algorithms.qft(28)
+def test_qft26_on_gaussian_state_vs_reference(threads):
+    init = W.gaussian_state(26, seed=26)
+    q = lq.algorithms.qft(26)
     want = threads.evolve_from(q, init)
     sv = lq.Statevector.from_numpy(init)
     lq.simulator.CompiledCircuit(q, True, 0, 0).apply(sv)
+    assert _host_maxdiff(sv.to_numpy(), want) < TOL
+
+
+def test_qft28_on_gaussian_state_equals_the_dft():
+    """QFT(n) with its final swaps is the discrete Fourier transform,
+    (QFT psi)_k = 2^(-n/2) sum_x e^{2 pi i x k / 2^n} psi_x — the known answer the
+    reference's own QFT test checks (tests/test_qft.cpp:30-69); numpy's inverse FFT
+    computes it (times 2^(n/2)) to ~1e-20 here."""
+    n = 28
+    init = W.gaussian_state(n, seed=n)
+    sv = lq.Statevector.from_numpy(init)
+    lq.simulator.CompiledCircuit(lq.algorithms.qft(n), True, 0, 0).apply(sv)
+    want = np.fft.ifft(init) * np.sqrt(float(1 << n))
     assert _host_maxdiff(sv.to_numpy(), want) < TOL
 
 
