@@ -7,13 +7,16 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .algorithms import adjoint_gradient
+from .algorithms import adjoint_gradient, batched_energy
 from .circuit import ParametricCircuit
 
 
 class AdjointExpectation(torch.autograd.Function):
-    """energies = E(params); params is (P,) or (B, P).  The gradient is computed together
-    with the energy in forward() and reused by backward()."""
+    """energies = E(params); params is (P,) or (B, P).  When the parameters need a
+    gradient it is computed together with the energy in forward() (the adjoint sweep shares
+    the forward pass) and reused by backward(); otherwise forward() runs only the batched
+    forward pass.  The parameter sets cross the C ABI as one host array (B x P doubles) and
+    the energies and gradients come back the same way."""
 
     @staticmethod
     def forward(ctx, params: torch.Tensor, ansatz: ParametricCircuit, hamiltonian,
@@ -21,13 +24,17 @@ class AdjointExpectation(torch.autograd.Function):
         p = params.detach().to("cpu", torch.float64).numpy()
         single = p.ndim == 1
         sets = p.reshape(1, -1) if single else p   # (B, P), also for P = 0
-        e, g = adjoint_gradient(hamiltonian, ansatz, sets, max_resident=max_resident)
-        grad = torch.as_tensor(np.asarray(g), dtype=params.dtype, device=params.device)
+        if ctx.needs_input_grad[0]:
+            e, g = adjoint_gradient(hamiltonian, ansatz, sets, max_resident=max_resident)
+            grad = torch.as_tensor(np.asarray(g), dtype=params.dtype, device=params.device)
+            if single:
+                grad = grad.reshape(-1)
+            ctx.save_for_backward(grad)
+        else:
+            e = batched_energy(hamiltonian, ansatz, sets, max_resident=max_resident)
         energies = torch.as_tensor(np.asarray(e), dtype=params.dtype, device=params.device)
         if single:
-            grad = grad.reshape(-1)
             energies = energies.reshape(())
-        ctx.save_for_backward(grad)
         return energies
 
     @staticmethod

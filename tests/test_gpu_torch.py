@@ -28,3 +28,20 @@ def test_autograd_single_and_batched(ref):
     for b in range(4):
         g = ref.parameter_shift_gradient(h, pc, sets[b])
         assert np.max(np.abs(tb.grad[b].cpu().numpy() - weights[b].item() * g)) < 1e-8
+
+
+def test_forward_without_gradient_runs_the_energy_pass_only(ref):
+    """Parameters that need no gradient: the energies equal the gradient path's and the
+    reference's, and nothing is saved for backward."""
+    pc, theta = W.random_pauli_ansatz(7, 12, seed=44, max_w=6)
+    h = W.random_hamiltonian(7, 15, seed=45)
+    sets = W.random_parameter_sets(pc.num_parameters(), 3, seed=46)
+    with torch.no_grad():
+        e0 = torch_ops.expectation(torch.tensor(sets, dtype=torch.float64), pc, h)
+    t = torch.tensor(sets, dtype=torch.float64, requires_grad=True)
+    e1 = torch_ops.expectation(t, pc, h)
+    assert not e0.requires_grad and e1.requires_grad
+    assert torch.max(torch.abs(e0 - e1.detach())).item() < 1e-12
+    for b in range(3):
+        want = ref.expectation(ref.run_statevector(pc.bind(sets[b])), h)
+        assert abs(e0[b].item() - want) < 1e-11
