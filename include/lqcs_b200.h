@@ -477,7 +477,8 @@ uint64_t lqcs_kernel_launch_count(void);
  * the kernel against the barrier model (warps independent between CTA barriers, threads of
  * a warp independent between warp barriers) for a grid of `grid` CTAs (with state == NULL
  * only the first `race_ctas` CTAs are walked).  sync_tiles: 2 = as the kernel runs (a
- * barrier between a CTA's tiles where a remap changes the warp bits), 1 = a barrier between
+ * barrier between a CTA's tiles where the last layout's warp bits differ from the first
+ * layout's), 1 = a barrier between
  * all tiles, 0 = none, 3 = the double-buffered kernel (LQCS_REG_PIPE=1; 2^11- and
  * 2^12-amplitude tiles); + 8 leaves out the barrier a relabelling pass puts between its
  * loads and stores.  *n_races counts racing accesses; `report` (capacity report_cap)

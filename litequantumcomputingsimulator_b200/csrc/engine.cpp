@@ -747,6 +747,9 @@ std::string program_key(const std::vector<GateDesc>& gates, uint32_t n, const Fu
     put(&tc.L, sizeof tc.L);
     put(&tc.inner, sizeof tc.inner);
     put(&reg, 1);
+    const uint8_t search = tc.search ? 1 : 0, mma = tc.mma ? 1 : 0;
+    put(&search, 1);
+    put(&mma, 1);
     for (const GateDesc& g : gates) {
         const uint64_t sizes[5] = {g.qubits.size(), g.params.size(), g.mat.size(), g.perm.size(),
                                    g.pauli.size()};

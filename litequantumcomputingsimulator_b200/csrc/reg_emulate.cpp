@@ -192,8 +192,8 @@ struct AmpLog {
 // Emulate one register pass on `in` (read) / `out` (written; `amps` records stores and
 // loading tiles) — values are skipped when in == nullptr — and check its shared-memory
 // accesses for every CTA of a grid of `grid` CTAs (only the first `race_ctas` CTAs when
-// values are skipped).  sync_tiles: 1 barrier between tiles, 0 none, 2 only where a remap
-// changes the warp bits (the pass's cta_remaps).
+// values are skipped).  sync_tiles: 1 barrier between tiles, 0 none, 2 as the pass says
+// (its sync_tiles: where the last layout's warp bits differ from the first's).
 //
 // pipe: the double-buffered kernel (k_regtile_pipe) instead: each tile's amplitudes arrive
 // by asynchronous copies into one of two shared buffers (issued right after the previous
@@ -206,7 +206,7 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                       uint64_t grid, uint64_t race_ctas, int sync_tiles, bool pipe,
                       bool drop_load_barrier, uint32_t pass_index, RaceLog& log) {
     RegPass p = pass;
-    p.sync_tiles = sync_tiles == 2 ? p.cta_remaps : static_cast<uint32_t>(sync_tiles != 0);
+    if (sync_tiles != 2) p.sync_tiles = static_cast<uint32_t>(sync_tiles != 0);
     const uint32_t m = p.m;
     const uint32_t kTB = m - kRegBits;
     const uint32_t kT = 1u << kTB;
@@ -326,12 +326,14 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                 for (uint32_t w = 0; w < (kT + 31) / 32; ++w) model.warp_barrier(w);
             }
             // operations, thread by thread between barriers: a remap is a barrier point, so
-            // each thread runs up to the next remap, then the remap's two phases follow
+            // each thread runs up to the next remap, then the remap's two phases follow; a
+            // tensor-path block (warp barrier, then one instruction of the whole warp) is
+            // such a point too
             std::vector<uint32_t> cur(kT, 0);
             uint32_t o = 0;
             while (o <= p.n_ops) {
                 uint32_t end = o;
-                while (end < p.n_ops && !(ops[end].kind == kRegRemap &&
+                while (end < p.n_ops && !((ops[end].kind == kRegRemap || ops[end].kind == kRegMma) &&
                                           (base & ops[end].gcmask) == ops[end].gcmask))
                     ++end;
                 // [o, end): non-remap operations, each thread independently
@@ -347,7 +349,8 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                             uint32_t sel = 0;
                             for (uint32_t q = 0; q < op.nsel; ++q)
                                 sel |= static_cast<uint32_t>((base >> op.selq[q]) & 1u) << q;
-                            const uint32_t k2 = op.kind == kRegDense ? 2u * op.k : op.k;
+                            const uint32_t k2 =
+                                op.kind == kRegDense || op.kind == kRegMma ? 2u * op.k : op.k;
                             moff += sel << k2;
                         }
                         if (op.kind == kRegDense) {
@@ -407,6 +410,41 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                     }
                 }
                 if (end >= p.n_ops) break;
+                if (ops[end].kind == kRegMma) {
+                    // every lane of a warp whose warp-bit controls are all 1 (lane controls
+                    // never occur: the lowering refuses them); register u's quad of lanes
+                    // 4g..4g+3 holds members 0..3 of group g, matrix bit j on lane bit j
+                    const RegOp& op = ops[end];
+                    uint32_t moff = op.mat_off;
+                    if (op.nsel) {
+                        uint32_t sel = 0;
+                        for (uint32_t q = 0; q < op.nsel; ++q)
+                            sel |= static_cast<uint32_t>((base >> op.selq[q]) & 1u) << q;
+                        moff += sel << (2u * op.k);
+                    }
+                    if (op.tcmask & 31u)
+                        logic("register tile emulation: a tensor-path block is controlled by a lane bit");
+                    for (uint32_t w = 0; w < (kT + 31) / 32; ++w) {
+                        const uint32_t t0 = 32 * w;
+                        if ((t0 & op.tcmask) != op.tcmask) continue;
+                        model.warp_barrier(w);
+                        if (!in) continue;
+                        for (uint32_t u = 0; u < kE; ++u) {
+                            if ((u & op.rcmask) != op.rcmask) continue;
+                            for (uint32_t g = 0; g < 8; ++g) {
+                                cd a[4], y[4];
+                                for (uint32_t k = 0; k < 4; ++k) a[k] = v[(t0 + 4 * g + k) * kE + u];
+                                for (uint32_t j = 0; j < 4; ++j) {
+                                    y[j] = 0;
+                                    for (uint32_t k = 0; k < 4; ++k) y[j] += mats[moff + 4 * j + k] * a[k];
+                                }
+                                for (uint32_t j = 0; j < 4; ++j) v[(t0 + 4 * g + j) * kE + u] = y[j];
+                            }
+                        }
+                    }
+                    o = end + 1;
+                    continue;
+                }
                 // the remap at `end`: write under the current layout, barrier, read under the
                 // new one, barrier
                 const RegOp& rm = ops[end];

@@ -278,6 +278,46 @@ __device__ __forceinline__ void reg_diag(double2 (&v)[kE], const RegOp& op, cons
     }
 }
 
+// d += a * b on the FP64 tensor path, one m8n8k4 step: lane l holds a = A[l / 4][l % 4],
+// b = B[l % 4][l / 4] and d = D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void mma_f64(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Two-qubit block on the lane pair (kRegMma), every register index whose control bits are
+// all 1.  For register u the warp's 32 amplitudes form A (8 groups on lanes 2..4 x 4 members
+// on lanes 0..1), split into real and imaginary parts; the 4 x 4 complex matrix M enters as
+// B with column n = 2 j + c holding output member j, part c: B_re[k][n] = c ? Im M[j][k] :
+// Re M[j][k], B_im[k][n] = c ? Re M[j][k] : -Im M[j][k].  D = A_re B_re + A_im B_im then
+// leaves (Re, Im) of the lane's own new amplitude in its two accumulators.  The whole warp
+// runs it (the caller keeps it converged); lane l loads one matrix entry.
+__device__ __forceinline__ void reg_mma(double2 (&v)[kE], uint32_t mat, uint32_t rcmask) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const double2 e = lds2(mat + 16u * (((lane >> 3) << 2) | (lane & 3u)));
+    const bool im_col = ((lane >> 2) & 1u) != 0;
+    const double b_re = im_col ? e.y : e.x, b_im = im_col ? e.x : -e.y;
+    if (rcmask == 0) {
+#pragma unroll
+        for (int u = 0; u < kE; ++u) {
+            double d0 = 0.0, d1 = 0.0;
+            mma_f64(d0, d1, v[u].x, b_re);
+            mma_f64(d0, d1, v[u].y, b_im);
+            v[u] = make_double2(d0, d1);
+        }
+        return;
+    }
+#pragma unroll
+    for (int u = 0; u < kE; ++u) {
+        if ((u & rcmask) != rcmask) continue;   // uniform over the warp
+        double d0 = 0.0, d1 = 0.0;
+        mma_f64(d0, d1, v[u].x, b_re);
+        mma_f64(d0, d1, v[u].y, b_im);
+        v[u] = make_double2(d0, d1);
+    }
+}
+
 __device__ __forceinline__ uint32_t thread_slot(const RegLayout& ly, uint32_t tbits) {
     uint32_t s = 0;
     for (uint32_t i = 0; i < tbits; ++i)
@@ -293,8 +333,12 @@ __device__ __forceinline__ uint64_t thread_goff(const RegLayout& ly, uint32_t tb
     return g;
 }
 
-// MINB resident CTAs per SM: registers per thread <= 65536 / (MINB * threads).
-template <int M, int MINB>
+// MINB resident CTAs per SM: registers per thread <= 65536 / (MINB * threads).  FMAD: the
+// pass has dense records on register bits (FP64 FMAs); MMA: it has tensor-path records.  A
+// kernel carries only the paths its pass uses: with both, the register allocation spills
+// (364 bytes at 128 registers against 64 for the FMA path alone and 8 for the tensor path
+// alone), so each pass runs the variant of its own records.
+template <int M, int MINB, bool FMAD, bool MMA>
 __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
 k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
           const RegLayout* __restrict__ layouts, const double2* __restrict__ mats) {
@@ -455,20 +499,29 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                 continue;
             }
             const uint32_t tc = op.tcmask;
-            if ((threadIdx.x & tc) != tc) continue;
-            const uint32_t rc = op.rcmask;
             uint32_t moff = op.mat_off;
             if (const uint32_t nsel = op.nsel) {   // matrix picked by the tile's selector bits
                 uint32_t sel = 0;
                 for (uint32_t i = 0; i < nsel; ++i)
                     sel |= static_cast<uint32_t>((base >> op.selq[i]) & 1u) << i;
-                const uint32_t k2 = kind == kRegDense ? 2u * op.k : op.k;
+                const uint32_t k2 = kind == kRegDense || kind == kRegMma ? 2u * op.k : op.k;
                 moff += sel << k2;
             }
+            if (kind == kRegMma) {
+                if constexpr (MMA) {
+                    // controls on warp bits only: the condition is the same on every lane
+                    if ((threadIdx.x & tc & ~31u) != (tc & ~31u)) continue;
+                    __syncwarp();
+                    reg_mma(v, smat_addr + 16u * moff, op.rcmask);
+                }
+                continue;
+            }
+            if ((threadIdx.x & tc) != tc) continue;
+            const uint32_t rc = op.rcmask;
             const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
                                                      : smat_addr + 16u * moff;
             if (kind == kRegDense) {
-                dispatch_dense(v, op.code, SharedMat{mat}, rc);
+                if constexpr (FMAD) dispatch_dense(v, op.code, SharedMat{mat}, rc);
             } else if (kind == kRegPhase) {
                 const double2 f = lds2(mat);
 #pragma unroll
@@ -679,16 +732,22 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
                 continue;
             }
             const uint32_t tc = op.tcmask;
-            if ((threadIdx.x & tc) != tc) continue;
-            const uint32_t rc = op.rcmask;
             uint32_t moff = op.mat_off;
             if (const uint32_t nsel = op.nsel) {
                 uint32_t sel = 0;
                 for (uint32_t i = 0; i < nsel; ++i)
                     sel |= static_cast<uint32_t>((base >> op.selq[i]) & 1u) << i;
-                const uint32_t k2 = kind == kRegDense ? 2u * op.k : op.k;
+                const uint32_t k2 = kind == kRegDense || kind == kRegMma ? 2u * op.k : op.k;
                 moff += sel << k2;
             }
+            if (kind == kRegMma) {
+                if ((threadIdx.x & tc & ~31u) != (tc & ~31u)) continue;   // uniform per warp
+                __syncwarp();
+                reg_mma(v, smat_addr + 16u * moff, op.rcmask);
+                continue;
+            }
+            if ((threadIdx.x & tc) != tc) continue;
+            const uint32_t rc = op.rcmask;
             const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
                                                      : smat_addr + 16u * moff;
             if (kind == kRegDense) {
@@ -731,11 +790,11 @@ void launch_pipe(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPas
     check_launch("register tile pass (double-buffered)");
 }
 
-template <int M, int MINB>
-void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
-               const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
+template <int M, int MINB, bool FMAD, bool MMA>
+void launch_mbf(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
+                const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
     constexpr uint32_t kT = 1u << (M - kRegBits);
-    auto kern = k_regtile<M, MINB>;
+    auto kern = k_regtile<M, MINB, FMAD, MMA>;
     cuda_check_launch_attr(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kTileMaxSmem)));
     static const size_t static_smem = [&] {
@@ -749,6 +808,14 @@ void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass&
     const uint32_t grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, p.n_tiles)));
     kern<<<dim3(grid, batch), kT, smem, ctx.stream>>>(st, p, d_ops, d_layouts, d_mats);
     check_launch("register tile pass");
+}
+
+template <int M, int MINB>
+void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
+               const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
+    if (!p.mma_ops) launch_mbf<M, MINB, true, false>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    else if (!p.fma_dense) launch_mbf<M, MINB, false, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    else launch_mbf<M, MINB, true, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
 }
 
 // Residency per tile size: about 160 registers per thread keep the dense paths free of

@@ -91,8 +91,14 @@ constexpr uint32_t kRegMaxDynTerms = 48;        // gated phase terms of one per-
 // kRegDiagDyn: a diagonal whose table is built at the start of every tile from a base table
 // and gated phase terms (the matrices hold the 2^k base entries, then per term its factor and
 // a word pair {out-of-tile mask, entry mask}); it is applied like kRegDiag.
+// kRegMma: a two-qubit dense block whose targets are the tile bits on lanes 0 and 1 (matrix
+// bit 0 on lane 0), applied with mma.sync.m8n8k4.f64 by the whole warp: over the reals the
+// 4 x 4 complex block is an 8 x 8 real matrix, each register index u of the warp's 32 lanes
+// a set of 8 groups (lanes 2..4) of 4 amplitudes (lanes 0..1), and two k = 4 steps (real
+// parts, then imaginary parts) give every lane its own new amplitude.  Its tile controls are
+// register bits (rcmask) or warp bits (tcmask), never lanes.
 enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4,
-                 kRegDiagDyn = 5 };
+                 kRegDiagDyn = 5, kRegMma = 6 };
 
 struct RegLayout {
     uint16_t rsw[kRegBits];   // tile_swizzle(1 << rpos[i])
@@ -135,6 +141,8 @@ struct RegPass {
     uint8_t store_qubit[kRegMaxBits];   // of qubit store_qubit[b]
     uint32_t load_barrier;    // a barrier between the tile's loads and stores is needed and no
                               // other barrier provides it (relabelled stores, in place)
+    uint32_t fma_dense;       // some record is a dense op on register bits (kRegDense)
+    uint32_t mma_ops;         // some record is a tensor-path block (kRegMma)
 };
 
 static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");

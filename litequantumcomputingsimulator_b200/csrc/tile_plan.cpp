@@ -39,6 +39,7 @@ TileConfig default_tile_config(uint32_t n) {
     c.inner = static_cast<uint32_t>(env_int("LQCS_TILE_INNER", 2));
     c.reg = env_int("LQCS_TILE_REG", 1) != 0;
     c.search = env_int("LQCS_TILE_SEARCH", 1) != 0;
+    c.mma = env_int("LQCS_REG_MMA", 0) != 0;
     c.m = std::max<uint32_t>(kTileMinBits, std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n));
     c.L = std::min<uint32_t>(std::min(c.L, c.m), kTileMinBits);   // column bits come from the thread index
     if (c.m - c.L > kTileMaxHigh) c.L = c.m - kTileMaxHigh;
@@ -842,19 +843,35 @@ Use op_use(const LocalOp& o) {
     return u;
 }
 
-// Scan of the pending ops under register set S: every op that commutes with all skipped
-// ops before it and whose dense targets are register bits is applied.  Returns the count;
-// with `emitted` the applied ops move there (in order) and `pending` keeps the rest.
+// A layout as the scheduler sees it: register set S, warp bits W and the pair P of tile
+// bits on lanes 0 and 1 (0: none), where the two-qubit blocks of a tensor-core pass run.
+struct Lay {
+    uint32_t S = 0, W = 0, P = 0;
+};
+
+// Whether op o runs in layout ly: a dense op on the tensor path (mma) needs its targets
+// (two, or one) on the lane pair and its tile controls on register or warp bits (every lane
+// of a warp takes part in the instruction); any other dense op needs its targets on
+// register bits.
+bool fits(const LocalOp& o, bool mma, const Lay& ly) {
+    if (o.kind != kTileDense) return true;
+    if (mma) return ly.P != 0 && (target_mask(o) & ~ly.P) == 0 && (o.lmask & ~(ly.S | ly.W)) == 0;
+    return (target_mask(o) & ~ly.S) == 0;
+}
+
+// Scan of the pending ops under layout ly: every op that commutes with all skipped ops
+// before it and fits the layout is applied.  Returns the count; with `emitted` the applied
+// ops move there (in order) and `pending` keeps the rest.  mma[i]: op i is a tensor-path op.
 size_t scan(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
-            std::vector<uint32_t>& pending, uint32_t S, std::vector<uint32_t>* emitted) {
+            const std::vector<uint8_t>& mma, std::vector<uint32_t>& pending, const Lay& ly,
+            std::vector<uint32_t>* emitted) {
     uint32_t busy_nd = 0, busy_dg = 0;
     size_t cnt = 0;
     std::vector<uint32_t> rest;
     for (uint32_t i : pending) {
         const Use& u = use[i];
         const bool blocked = (u.nd & (busy_nd | busy_dg)) != 0 || (u.dg & busy_nd) != 0;
-        const bool fits = ops[i].kind != kTileDense || (target_mask(ops[i]) & ~S) == 0;
-        if (!blocked && fits) {
+        if (!blocked && fits(ops[i], mma[i] != 0, ly)) {
             ++cnt;
             if (emitted) emitted->push_back(i);
         } else {
@@ -867,30 +884,45 @@ size_t scan(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
     return cnt;
 }
 
-// Dense ops of `pending` whose targets all lie in S (a tie-break: later use of a layout).
-size_t covered(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pending, uint32_t S) {
+// Register-path dense ops of `pending` whose targets all lie in S (a tie-break: later use
+// of a layout).
+size_t covered(const std::vector<LocalOp>& ops, const std::vector<uint8_t>& mma,
+               const std::vector<uint32_t>& pending, uint32_t S) {
     size_t c = 0;
     for (uint32_t i : pending)
-        if (ops[i].kind == kTileDense && (target_mask(ops[i]) & ~S) == 0) ++c;
+        if (ops[i].kind == kTileDense && !mma[i] && (target_mask(ops[i]) & ~S) == 0) ++c;
     return c;
 }
 
-// Layout of register set S and warp bits W on an m-bit tile.  Thread-index bits 0..4 (the
-// lanes) take the tile bits outside S and W, bits 5.. (the warps) take W in ascending order.
-// Lanes ascending, except that when they are not tile bits 0..4 the first three are picked
-// with distinct residues mod 3: tile_swizzle sends 1 << b to slot bit (b mod 3), so then the
-// 8 lanes of a quarter warp hit 8 different 16-byte bank groups in a remap.  A remap that
-// keeps W keeps every warp on the same tile indices, hence on its own shared-memory slots:
-// it needs only a warp-level barrier.
-RegLayout make_layout(uint32_t S, uint32_t W, uint32_t m) {
+// Layout of register set S, warp bits W and lane pair P on an m-bit tile.  Thread-index bits
+// 0..4 (the lanes) take the tile bits outside S and W, bits 5.. (the warps) take W in
+// ascending order.  With a pair, lanes 0 and 1 take its lower and higher bit and lane 2 a
+// bit of the third residue mod 3 where one exists; otherwise lanes ascending, except that
+// when they are not tile bits 0..4 the first three are picked with distinct residues mod 3:
+// tile_swizzle sends 1 << b to slot bit (b mod 3), so then the 8 lanes of a quarter warp hit
+// 8 different 16-byte bank groups in a remap.  A remap that keeps W keeps every warp on the
+// same tile indices, hence on its own shared-memory slots: it needs only a warp-level
+// barrier.
+RegLayout make_layout(uint32_t S, uint32_t W, uint32_t m, uint32_t P = 0) {
     RegLayout ly{};
     std::vector<uint32_t> rb, lanes, warps;
     for (uint32_t b = 0; b < m; ++b) {
         if ((S >> b) & 1) rb.push_back(b);
         else if ((W >> b) & 1) warps.push_back(b);
-        else lanes.push_back(b);
+        else if (!((P >> b) & 1)) lanes.push_back(b);
     }
-    if (lanes.size() >= 3 && lanes[0] + lanes.size() - 1 != lanes.back()) {
+    if (P != 0) {
+        const uint32_t p0 = static_cast<uint32_t>(__builtin_ctz(P));
+        const uint32_t p1 = 31u - static_cast<uint32_t>(__builtin_clz(P));
+        const uint32_t seen = (1u << (p0 % 3)) | (1u << (p1 % 3));
+        for (size_t i = 0; i < lanes.size(); ++i)
+            if (!((seen >> (lanes[i] % 3)) & 1)) {
+                std::rotate(lanes.begin(), lanes.begin() + static_cast<long>(i),
+                            lanes.begin() + static_cast<long>(i) + 1);
+                break;
+            }
+        lanes.insert(lanes.begin(), {p0, p1});
+    } else if (lanes.size() >= 3 && lanes[0] + lanes.size() - 1 != lanes.back()) {
         std::vector<uint32_t> first, rest;
         uint32_t seen = 0;
         for (uint32_t b : lanes) {
@@ -928,7 +960,7 @@ bool residues_spread(uint32_t lanes) {
 // `count` warp bits out of `avail`: the tile bits the pending dense operations target least
 // (ties: the higher bit), so that few later operations need a bit that is a warp bit.
 uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint32_t>& pending,
-                        uint32_t avail, uint32_t count) {
+                        uint32_t avail, uint32_t count, uint32_t pair = 0) {
     uint32_t usage[32] = {};
     for (uint32_t i : pending)
         if (ops[i].kind == kTileDense)
@@ -942,14 +974,15 @@ uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint3
         }
         if (best >= 0) W |= 1u << best;
     }
-    // lanes without a residue mod 3: trade a warp bit for a lane bit as little used
-    if (!residues_spread(avail & ~W)) {
+    // lanes (the rest of avail and the lane pair) without a residue mod 3: trade a warp bit
+    // for a lane bit as little used
+    if (!residues_spread((avail & ~W) | pair)) {
         for (uint32_t w = 0; w < 32; ++w) {
             if (!((W >> w) & 1)) continue;
             for (uint32_t l = 0; l < 32; ++l) {
                 const uint32_t W2 = (W & ~(1u << w)) | (1u << l);
                 if (((avail & ~W) >> l) & 1 && usage[l] <= usage[w] &&
-                    residues_spread(avail & ~W2))
+                    residues_spread((avail & ~W2) | pair))
                     return W2;
             }
         }
@@ -958,12 +991,14 @@ uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint3
 }
 
 // Register sets of size kRegBits inside `allowed` that contain `must`, best first by
-// (ops applied now, dense ops covered later, usable as the final layout, and — when the
-// warp bits are known, `lane_pool` being the tile bits outside them — lanes that take all
-// three residues mod 3, which keeps the remaps free of bank conflicts).
+// (ops applied now with warp bits W and lane pair P, register-path dense ops covered later,
+// usable as the final layout, and — when the warp bits are known, `lane_pool` being the
+// tile bits outside them — lanes that take all three residues mod 3, which keeps the remaps
+// free of bank conflicts).
 uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use,
-                    std::vector<uint32_t>& pending, uint32_t must, uint32_t allowed, uint32_t m,
-                    uint32_t lane_pool = 0) {
+                    const std::vector<uint8_t>& mma, std::vector<uint32_t>& pending,
+                    uint32_t must, uint32_t allowed, uint32_t m, uint32_t lane_pool = 0,
+                    uint32_t P = 0, uint32_t W = 0) {
     uint32_t best = 0;
     size_t best_now = 0, best_later = 0;
     bool best_final = false, best_spread = false, have = false;
@@ -972,8 +1007,8 @@ uint32_t choose_set(const std::vector<LocalOp>& ops, const std::vector<Use>& use
         if (__builtin_popcount(S) != static_cast<int>(kRegBits) || (S & must) != must ||
             (S & ~allowed) != 0)
             continue;
-        const size_t now = scan(ops, use, pending, S, nullptr);
-        const size_t later = covered(ops, pending, S);
+        const size_t now = scan(ops, use, mma, pending, Lay{S, W, P}, nullptr);
+        const size_t later = covered(ops, mma, pending, S);
         const bool fin = (S & lanes) == 0;
         const bool spread = lane_pool != 0 && residues_spread(lane_pool & ~S);
         const auto key = std::make_tuple(now, later, fin, spread);
@@ -996,7 +1031,33 @@ namespace {
 // Matrix data of op o in layout (ly, S): dense matrices re-indexed so that matrix bit q is
 // the q-th lowest register target (one block per selector value), diagonals and phase
 // factors as they are.  X operations (swaps) have none.
-void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vector<cd>& mats) {
+// A tensor-path op (mma) instead: matrix bit 0 is the tile bit on lane 0, bit 1 the one on
+// lane 1.
+void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vector<cd>& mats,
+                     bool mma = false) {
+    if (mma) {
+        std::vector<cd> pm(16);
+        if (o.lt.size() == 1) {   // one target: the 2 x 2 matrix on its lane, identity on the other
+            const uint32_t j = o.lt[0] == ly.tpos[0] ? 0u : 1u;
+            for (size_t blk = 0; blk < o.m.size(); blk += 4) {
+                for (uint32_t rr = 0; rr < 4; ++rr)
+                    for (uint32_t cc = 0; cc < 4; ++cc)
+                        pm[rr * 4 + cc] = ((rr ^ cc) >> (1u - j)) & 1u
+                                              ? cd{0, 0}
+                                              : o.m[blk + ((rr >> j) & 1u) * 2 + ((cc >> j) & 1u)];
+                mats.insert(mats.end(), pm.begin(), pm.end());
+            }
+            return;
+        }
+        const bool swap = o.lt[0] != ly.tpos[0];   // matrix bit 0 is on lane 1
+        auto sw = [&](uint32_t l) { return swap ? ((l & 1u) << 1) | (l >> 1) : l; };
+        for (size_t blk = 0; blk < o.m.size(); blk += 16) {
+            for (uint32_t rr = 0; rr < 4; ++rr)
+                for (uint32_t cc = 0; cc < 4; ++cc) pm[sw(rr) * 4 + sw(cc)] = o.m[blk + rr * 4 + cc];
+            mats.insert(mats.end(), pm.begin(), pm.end());
+        }
+        return;
+    }
     if (o.kind == kTilePhase || o.kind == kTileDiag) {
         mats.insert(mats.end(), o.m.begin(), o.m.end());
         // per-tile terms: the factor, then {gcmask low 32 bits, gcmask high 32 bits * 64 +
@@ -1039,8 +1100,10 @@ void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vec
     }
 }
 
-// The record of op o in layout (ly, S); its matrices start at mat_off.
-RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m, uint32_t mat_off) {
+// The record of op o in layout (ly, S); its matrices start at mat_off.  mma: a two-qubit
+// block on the lane pair (tensor path), its controls on register or warp bits.
+RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m, uint32_t mat_off,
+                  bool mma = false) {
     int ridx[32], tidx[32];
     for (uint32_t i = 0; i < kRegBits; ++i) ridx[ly.rpos[i]] = static_cast<int>(i);
     for (uint32_t i = 0; i < m - kRegBits; ++i) tidx[ly.tpos[i]] = static_cast<int>(i);
@@ -1056,7 +1119,12 @@ RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m,
     }
     const uint32_t k = static_cast<uint32_t>(o.lt.size());
     r.k = static_cast<uint8_t>(k);
-    if (o.kind == kTilePhase) {
+    if (mma) {
+        if (r.tcmask & ((1u << kLaneBits) - 1u))
+            logic("register tile lowering: a tensor-path block is controlled by a lane bit");
+        r.kind = kRegMma;
+        r.k = 2;   // always a 4 x 4 block (a one-target op with the identity on the other lane)
+    } else if (o.kind == kTilePhase) {
         r.kind = kRegPhase;
     } else if (o.kind == kTileDiag) {
         r.kind = o.dyn.empty() ? kRegDiag : kRegDiagDyn;
@@ -1096,16 +1164,29 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             return false;
     std::vector<Use> use;
     for (const LocalOp& o : ops) use.push_back(op_use(o));
+    // One- and two-target dense blocks run on the FP64 tensor path (lane pair) when cfg.mma
+    // is set — all but X operations, which stay register swaps; their tile controls must fit
+    // on the register bits, which at most kRegBits can.
+    std::vector<uint8_t> mma(ops.size(), 0);
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const LocalOp& o = ops[i];
+        const size_t k = o.lt.size();
+        const bool swapx = k == 1 && !o.variant && o.sel.empty() && is_x(o.m);
+        mma[i] = cfg.mma && o.kind == kTileDense && (k == 2 || (k == 1 && !swapx)) &&
+                 __builtin_popcount(o.lmask) <= static_cast<int>(kRegBits);
+    }
 
     std::vector<RegLayout> lays;
-    std::vector<uint32_t> lay_sets, lay_warps;
-    auto layout_index = [&](uint32_t S, uint32_t W) {
-        for (size_t i = 0; i < lay_sets.size(); ++i)
-            if (lay_sets[i] == S && lay_warps[i] == W) return static_cast<uint32_t>(i);
-        lay_sets.push_back(S);
-        lay_warps.push_back(W);
-        lays.push_back(make_layout(S, W, m));
-        return static_cast<uint32_t>(lay_sets.size() - 1);
+    std::vector<Lay> lay_keys;
+    auto layout_index = [&](uint32_t S, uint32_t W, uint32_t P) {
+        if ((P != 0 && __builtin_popcount(P) != 2) || (P & (S | W)) != 0 || (S & W) != 0)
+            logic("register tile lowering: inconsistent layout");
+        for (size_t i = 0; i < lay_keys.size(); ++i)
+            if (lay_keys[i].S == S && lay_keys[i].W == W && lay_keys[i].P == P)
+                return static_cast<uint32_t>(i);
+        lay_keys.push_back(Lay{S, W, P});
+        lays.push_back(make_layout(S, W, m, P));
+        return static_cast<uint32_t>(lay_keys.size() - 1);
     };
     // schedule: (op, layout) in application order, remaps as (-1 warp-local / -2 CTA-wide,
     // new layout)
@@ -1116,25 +1197,70 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     const uint32_t nwarp = m - kRegBits - kLaneBits;
     std::vector<uint32_t> pending(ops.size());
     for (uint32_t i = 0; i < ops.size(); ++i) pending[i] = i;
+    // Lane pair for tensor-path op i out of the tile bits `pool` (0: none there): its two
+    // targets; for one target, the targets of a pending two-target block that contains it,
+    // else the target and the lowest free bit of pool (one of `prefer` if there is one).
+    auto pair_for = [&](uint32_t i, uint32_t pool, uint32_t prefer) -> uint32_t {
+        const uint32_t t = target_mask(ops[i]);
+        if ((t & ~pool) != 0) return 0u;
+        if (ops[i].lt.size() == 2) return t;
+        for (uint32_t j : pending) {
+            const uint32_t tj = target_mask(ops[j]);
+            if (mma[j] && ops[j].lt.size() == 2 && (tj & t) && !(tj & ~pool) && !(tj & ops[i].lmask))
+                return tj;
+        }
+        const uint32_t free = pool & ~t & ~ops[i].lmask;
+        if (free == 0) return 0u;
+        const uint32_t pick = (free & prefer) ? (free & prefer) : free;
+        return t | (1u << __builtin_ctz(pick));
+    };
+    // lane pair for a layout whose lanes are `pool`: that of the first pending tensor-path
+    // block that has one there
+    auto next_pair = [&](uint32_t pool) -> uint32_t {
+        for (uint32_t i : pending)
+            if (mma[i])
+                if (const uint32_t pr = pair_for(i, pool, pool)) return pr;
+        return 0u;
+    };
     // the first layout loads the tile: lanes on tile bits 0..4 keep the loads coalesced
-    uint32_t S = choose_set(ops, use, pending, 0, high, m);
-    uint32_t W = pick_warp_bits(ops, pending, high & ~S, nwarp);
-    uint32_t cur = layout_index(S, W);
+    uint32_t P = next_pair(lanes);
+    uint32_t S = choose_set(ops, use, mma, pending, 0, high, m, 0, P, 0);
+    uint32_t W = pick_warp_bits(ops, pending, high & ~S, nwarp, P);
+    uint32_t cur = layout_index(S, W, P);
     bool sync_tiles = false;
     while (true) {
         std::vector<uint32_t> applied;
-        scan(ops, use, pending, S, &applied);
+        scan(ops, use, mma, pending, Lay{S, W, P}, &applied);
         for (uint32_t i : applied) seq.emplace_back(static_cast<int>(i), cur);
         if (pending.empty()) break;
-        const uint32_t must = target_mask(ops[pending.front()]);
+        const LocalOp& f = ops[pending.front()];
+        if (mma[pending.front()]) {   // a tensor-path block: its targets become the lane pair
+            P = pair_for(pending.front(), all, all & ~W);
+            if ((P & W) == 0) {       // warp-local: the warp bits stay
+                S = choose_set(ops, use, mma, pending, f.lmask & ~W, all & ~W & ~P, m, all & ~W,
+                               P, W);
+                cur = layout_index(S, W, P);
+                seq.emplace_back(-1, cur);
+            } else {                  // a target is a warp bit: new warp bits, CTA-wide remap
+                S = choose_set(ops, use, mma, pending, f.lmask, all & ~P, m, 0, P, 0);
+                W = pick_warp_bits(ops, pending, all & ~S & ~P, nwarp, P);
+                cur = layout_index(S, W, P);
+                seq.emplace_back(-2, cur);
+                sync_tiles = true;
+            }
+            continue;
+        }
+        const uint32_t must = target_mask(f);
         if ((must & W) == 0) {   // warp-local: the warp bits stay
-            S = choose_set(ops, use, pending, must, all & ~W, m, all & ~W);
-            cur = layout_index(S, W);
+            S = choose_set(ops, use, mma, pending, must, all & ~W, m, all & ~W, 0, W);
+            P = next_pair(all & ~W & ~S);
+            cur = layout_index(S, W, P);
             seq.emplace_back(-1, cur);
         } else {                 // a target is a warp bit: new warp bits, CTA-wide remap
-            S = choose_set(ops, use, pending, must, all, m);
-            W = pick_warp_bits(ops, pending, all & ~S, nwarp);
-            cur = layout_index(S, W);
+            S = choose_set(ops, use, mma, pending, must, all, m);
+            P = next_pair(all & ~S);
+            W = pick_warp_bits(ops, pending, all & ~S & ~P, nwarp, P);
+            cur = layout_index(S, W, P);
             seq.emplace_back(-2, cur);
             sync_tiles = true;
         }
@@ -1150,13 +1276,13 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     const uint32_t shigh = all & ~slanes;
     if (((S | W) & slanes) != 0) {
         if ((W & slanes) == 0) {
-            seq.emplace_back(-1, layout_index(shigh & ~W, W));
+            seq.emplace_back(-1, layout_index(shigh & ~W, W, 0));
         } else {
             uint32_t Sf = 0;   // the four highest tile bits outside the store lanes
             for (int b = static_cast<int>(m) - 1; b >= 0 && __builtin_popcount(Sf) < static_cast<int>(kRegBits); --b)
                 if ((shigh >> b) & 1) Sf |= 1u << b;
             W = pick_warp_bits(ops, pending, shigh & ~Sf, nwarp);
-            seq.emplace_back(-2, layout_index(Sf, W));
+            seq.emplace_back(-2, layout_index(Sf, W, 0));
             sync_tiles = true;
         }
     }
@@ -1175,14 +1301,15 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             rec.push_back(r);
             continue;
         }
-        RegOp r = make_record(ops[i], lays[l], lay_sets[l], m, static_cast<uint32_t>(mats.size()));
+        RegOp r = make_record(ops[i], lays[l], lay_keys[l].S, m, static_cast<uint32_t>(mats.size()),
+                              mma[i] != 0);
         if (r.kind == kRegDiagDyn) {
             r.dyn_off = static_cast<uint16_t>(dyn_entries);
             dyn_entries += 1u << r.k;
             dyn_rec.push_back(static_cast<uint32_t>(rec.size()));
         }
         rec.push_back(r);
-        append_matrices(ops[i], lays[l], lay_sets[l], mats);
+        append_matrices(ops[i], lays[l], lay_keys[l].S, mats, mma[i] != 0);
     }
     if (rec.size() > kRegMaxRecords || lays.size() > kRegMaxLayouts || mats.size() > kRegMaxMatrix ||
         dyn_rec.size() > kRegMaxDyn || dyn_entries > kRegMaxDynEntries)
@@ -1200,7 +1327,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
                 if (!same_shape(ops[i], ob[i])) return false;
             const size_t before = mats.size();
             for (const auto& [i, l] : seq)
-                if (i >= 0) append_matrices(ob[i], lays[l], lay_sets[l], mats);
+                if (i >= 0) append_matrices(ob[i], lays[l], lay_keys[l].S, mats, mma[i] != 0);
             if (mats.size() - before != n_mat) return false;
         }
     }
@@ -1213,14 +1340,19 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     pass.n_layouts = static_cast<uint32_t>(lays.size());
     pass.n_mat = static_cast<uint32_t>(n_mat);
     pass.mat_stride = state_slots ? static_cast<uint32_t>(n_mat) : 0u;
-    // A barrier between a CTA's tiles only where some remap changes the warp bits: then a
-    // warp's shared-memory slots in the last layout of one tile are not its slots in the first
-    // layout of the next.  Where every remap keeps them, each warp only ever touches its own
-    // slots (tile_swizzle is linear and the warp bits are the same high tile bits in every
-    // layout), so no warp can overtake another into shared memory that one still uses; the
-    // host emulation (reg_emulate.cpp) checks this against the barrier model.
-    pass.sync_tiles = sync_tiles ? 1u : 0u;
-    pass.cta_remaps = pass.sync_tiles;
+    // A barrier between a CTA's tiles only where the last layout's warp bits differ from the
+    // first's: then a warp's shared-memory slots at the end of one tile are not its slots at
+    // the start of the next.  The slots a warp touches in a layout depend only on the warp
+    // bits and the warp's index (tile_swizzle is a linear bijection, and a layout only permutes
+    // the other bits among lanes and registers), so where they agree each warp meets only its
+    // own slots across the tile boundary — up to the next tile's first CTA-wide remap, whose
+    // barrier every warp reaches only after finishing this tile.  The host emulation
+    // (reg_emulate.cpp) checks this against the barrier model.
+    uint32_t last_layout = 0;
+    for (const auto& [i, l] : seq)
+        if (i < 0) last_layout = l;
+    pass.cta_remaps = sync_tiles ? 1u : 0u;
+    pass.sync_tiles = sync_tiles && lay_keys[last_layout].W != lay_keys[0].W ? 1u : 0u;
     for (uint32_t b = 0; b < m; ++b) {
         pass.store_qubit[b] = static_cast<uint8_t>(store_q[b]);
         const uint32_t home = b < cfg.L ? b : item.hbits[b - cfg.L];
@@ -1233,6 +1365,11 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     // the per-tile table barrier, both after the loads, order them; otherwise the kernel
     // adds a barrier after the loads.
     pass.load_barrier = pass.relabel && !sync_tiles && dyn_rec.empty() ? 1u : 0u;
+    pass.fma_dense = pass.mma_ops = 0;
+    for (const RegOp& r : rec) {
+        if (r.kind == kRegDense) pass.fma_dense = 1;
+        if (r.kind == kRegMma) pass.mma_ops = 1;
+    }
     for (size_t d = 0; d < dyn_rec.size(); ++d) pass.dyn_rec[d] = static_cast<uint8_t>(dyn_rec[d]);
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());
     layouts_out.insert(layouts_out.end(), lays.begin(), lays.end());

@@ -14,6 +14,9 @@ struct TileConfig {
     uint32_t inner = 2;    // widest dense operation fused inside a pass
     bool reg = true;       // register tile kernel where the pass fits it
     bool search = true;    // local search over each pass's high qubits (LQCS_TILE_SEARCH=0: off)
+    bool mma = false;      // register passes: one- and two-qubit blocks on the FP64 tensor
+                           // path (mma.sync m8n8k4) instead of FP64 FMAs over register bits
+                           // (LQCS_REG_MMA=1)
 };
 TileConfig default_tile_config(uint32_t n);
 

@@ -19,14 +19,15 @@ GREEDY = 1
 
 @pytest.fixture
 def tile_env():
-    keys = ("LQCS_TILE_BITS", "LQCS_TILE_LOW", "LQCS_TILE_INNER", "LQCS_TILE_REG")
+    keys = ("LQCS_TILE_BITS", "LQCS_TILE_LOW", "LQCS_TILE_INNER", "LQCS_TILE_REG", "LQCS_REG_MMA")
     saved = {k: os.environ.get(k) for k in keys}
 
-    def set_cfg(m, low, inner, reg=1):
+    def set_cfg(m, low, inner, reg=1, mma=0):
         os.environ["LQCS_TILE_BITS"] = str(m)
         os.environ["LQCS_TILE_LOW"] = str(low)
         os.environ["LQCS_TILE_INNER"] = str(inner)
         os.environ["LQCS_TILE_REG"] = str(reg)
+        os.environ["LQCS_REG_MMA"] = str(mma)
 
     yield set_cfg
     for k, v in saved.items():
@@ -183,10 +184,10 @@ def test_greedy_blocks_at_tile_sizes(port, n):
         assert np.max(np.abs(sv.to_numpy() - want)) < TOL
 
 
-@pytest.mark.parametrize("reg", [1, 0])
-def test_tile_batch_of_states(port, tile_env, reg):
-    """Tile passes walk a batch of states (gridDim.y)."""
-    tile_env(12, 5, 2, reg)
+@pytest.mark.parametrize("reg,mma", [(1, 0), (0, 0), (1, 1)])
+def test_tile_batch_of_states(port, tile_env, reg, mma):
+    """Tile passes walk a batch of states (gridDim.y), register passes on either path."""
+    tile_env(12, 5, 2, reg, mma)
     from litequantumcomputingsimulator_b200 import _native as N
     import ctypes as C
     n, batch = 13, 3
@@ -266,3 +267,22 @@ def test_autotune_picks_a_timed_plan_and_mode5_uses_it(port):
     prog.apply(sv)
     assert np.max(np.abs(sv.to_numpy() - want)) < TOL
     assert prog.n_ops == best["n_ops"]
+
+
+@pytest.mark.parametrize("m", [9, 11, 12, 13])
+def test_register_passes_on_the_tensor_path(port, ref, tile_env, m):
+    """LQCS_REG_MMA=1: one- and two-qubit blocks of register passes on mma.sync.m8n8k4.f64
+    (their targets on lanes 0 and 1) — every gate type with controls, the brickwork against
+    the reference, QFT on a Gaussian state, and a batch of states."""
+    tile_env(m, 5, 2, 1, 1)
+    for n, seed in ((13, 3), (16, 4)):
+        init = W.gaussian_state(n, seed=seed)
+        qc = random_circuit(n, 120, seed=seed, max_controls=4, max_unitary=3)
+        want = port.run_statevector(qc, fuse=False, state=init)
+        assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+    qc = W.brickwork(18, 12, seed=77)
+    assert all(k == 7 for k in kernel_kinds(qc))
+    assert np.max(np.abs(run(qc, TILE) - ref.run_statevector(qc, fuse=True))) < TOL
+    init = W.gaussian_state(16, seed=5)
+    q = lq.algorithms.qft(16)
+    assert np.max(np.abs(run(q, TILE, init) - ref.evolve_from(q, init))) < TOL

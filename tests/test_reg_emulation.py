@@ -5,7 +5,9 @@ checked against the CUDA barrier model.  No GPU.
 
 * Values: brickwork, QFT, partial inverse QFT and random circuits of the gate types that
   run inside register passes match the oracle within 1e-12, out of place, with every
-  amplitude stored exactly once by the tile that loaded it.
+  amplitude stored exactly once by the tile that loaded it — with two-qubit blocks on the
+  FP64 tensor path (the lane pair, emulated as the warp's mma.sync computes them) and on
+  register bits (LQCS_REG_MMA=0).
 * Races: none in the kernels as launched (a barrier between tiles only in passes whose
   remaps change the warp bits — elsewhere each warp keeps its own shared-memory slots from
   tile to tile; the double-buffered kernel), and many when that barrier is dropped from
@@ -86,9 +88,11 @@ def circuits():
     yield "random16", tile_circuit(16, 200, seed=6)
 
 
+@pytest.mark.parametrize("mma", ["1", "0"], ids=["tensor_path", "fma_path"])
 @pytest.mark.parametrize("mode", [PLANNED, BARRIER, PIPE])
 @pytest.mark.parametrize("name,qc", list(circuits()), ids=[c[0] for c in circuits()])
-def test_emulated_passes_match_oracle(port, name, qc, mode):
+def test_emulated_passes_match_oracle(port, monkeypatch, name, qc, mode, mma):
+    monkeypatch.setenv("LQCS_REG_MMA", mma)
     n = qc.num_qubits()
     init = W.gaussian_state(n, seed=n)
     got, passes, races, report = emulate(qc, mode, init)
@@ -119,10 +123,14 @@ def test_partial_inverse_qft_barrier_model(n, k):
         assert races == 0, (mode, report)
 
 
-def test_race_check_is_sensitive():
-    """Passes whose CTA-wide remaps change the warp bits need the barrier between tiles:
-    without it the check must report races; with it (or as planned), none."""
-    qc = W.brickwork(22, 10, seed=2025)
+@pytest.mark.parametrize("mma,n,seed", [("1", 23, 11), ("0", 22, 2025)],
+                         ids=["tensor_path", "fma_path"])
+def test_race_check_is_sensitive(monkeypatch, mma, n, seed):
+    """Passes whose last layout has other warp bits than the first need the barrier between
+    tiles: without it the check must report races; with it (or as planned), none.  Both
+    planners: two-qubit blocks on the lane pair (tensor path) and on register bits."""
+    monkeypatch.setenv("LQCS_REG_MMA", mma)
+    qc = W.brickwork(n, 10, seed=seed)
     _st, _p, races, report = emulate(qc, NONE, race_ctas=2)
     assert races > 0 and "races with" in report
     for mode in (PLANNED, BARRIER, PIPE):
