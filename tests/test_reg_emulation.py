@@ -8,10 +8,10 @@ checked against the CUDA barrier model.  No GPU.
   amplitude stored exactly once by the tile that loaded it — with two-qubit blocks on the
   FP64 tensor path (the lane pair, emulated as the warp's mma.sync computes them) and on
   register bits (LQCS_REG_MMA=0).
-* Races: none in the kernels as launched (a barrier between tiles only in passes whose
-  remaps change the warp bits — elsewhere each warp keeps its own shared-memory slots from
-  tile to tile; the double-buffered kernel), and many when that barrier is dropped from
-  passes that do change them — the check is sensitive.
+* Races: none in the kernels as launched (a barrier between tiles only in passes whose last
+  layout has other warp bits than the first — elsewhere each warp keeps its own
+  shared-memory slots across the tile boundary; the double-buffered kernel), and many when
+  that barrier is dropped from passes that need it — the check is sensitive.
 * In place: a pass that relabels tile bits (SWAPs of two tile qubits) stores amplitudes to
   places other warps load.  Without a barrier between the tile's loads and its stores a fast
   warp can overwrite an amplitude before a slow warp has read it; this made QFT(n >= 24)
