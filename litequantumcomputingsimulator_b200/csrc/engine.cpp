@@ -267,12 +267,30 @@ static Program assemble_tiles(const std::vector<GateDesc>& gates, uint32_t n,
                 continue;
             }
         }
-        TilePass tp;
-        p.pass_op_off.push_back(p.tile_ops.size());
-        lower_pass(it, gates, cfg, tp, p.tile_ops, p.tile_mats, &op.tile_flops);
-        op.pass_index = static_cast<uint32_t>(p.passes.size());
-        p.passes.push_back(tp);
-        ops.push_back(std::move(op));
+        // the shared-memory kernel: its operations have no native Pauli rotation, so the pass
+        // splits at each (the rotation runs on its own, the gates between as passes)
+        auto smem_pass = [&](const PlanItem& part) {
+            DevOp sop = op;
+            sop.src_gates = static_cast<uint32_t>(part.gates.size());
+            TilePass tp;
+            p.pass_op_off.push_back(p.tile_ops.size());
+            lower_pass(part, gates, cfg, tp, p.tile_ops, p.tile_mats, &sop.tile_flops);
+            sop.pass_index = static_cast<uint32_t>(p.passes.size());
+            p.passes.push_back(tp);
+            ops.push_back(std::move(sop));
+        };
+        PlanItem part = it;
+        part.gates.clear();
+        for (uint32_t gi : it.gates) {
+            if (!native_pauli(gates[gi], cfg)) {
+                part.gates.push_back(gi);
+                continue;
+            }
+            if (!part.gates.empty()) smem_pass(part);
+            part.gates.clear();
+            ops.push_back(lower_gate(gates[gi], n));
+        }
+        if (!part.gates.empty()) smem_pass(part);
     }
     return p;
 }

@@ -342,6 +342,33 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                     for (uint32_t i = o; i < end; ++i) {
                         const RegOp& op = ops[i];
                         if ((base & op.gcmask) != op.gcmask) continue;
+                        if (op.kind == kRegPauli) {   // rcmask / tcmask: Z-type bits
+                            if (!in) continue;
+                            const cd c = mats[op.mat_off];
+                            cd y = mats[op.mat_off + 1];
+                            const cd zd = mats[op.mat_off + 2];
+                            const uint64_t zg = static_cast<uint64_t>(zd.real()) |
+                                                (static_cast<uint64_t>(zd.imag()) << 32);
+                            if ((__builtin_popcountll(base & zg) + __builtin_popcount(t & op.tcmask)) & 1)
+                                y = -y;
+                            auto sign = [&](uint32_t u) {
+                                return (__builtin_popcount(u & op.rcmask) & 1) ? -1.0 : 1.0;
+                            };
+                            const uint32_t xr = op.code;
+                            if (xr == 0) {
+                                for (uint32_t u = 0; u < kE; ++u) vt[u] *= c + sign(u) * y;
+                                continue;
+                            }
+                            const uint32_t low = xr & (~xr + 1u);
+                            for (uint32_t u = 0; u < kE; ++u) {
+                                if (u & low) continue;
+                                const uint32_t w = u ^ xr;
+                                const cd a = vt[u], b = vt[w];
+                                vt[u] = c * a + sign(u) * y * b;
+                                vt[w] = c * b + sign(w) * y * a;
+                            }
+                            continue;
+                        }
                         if ((t & op.tcmask) != op.tcmask) continue;
                         const uint32_t rc = op.rcmask;
                         uint32_t moff = op.mat_off;

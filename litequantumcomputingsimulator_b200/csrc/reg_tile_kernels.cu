@@ -318,6 +318,56 @@ __device__ __forceinline__ void reg_mma(double2 (&v)[kE], uint32_t mat, uint32_t
     }
 }
 
+// Pauli rotation whose flip is the single register bit XR (kRegPauli after the reduction in
+// reg_pauli): amplitude u becomes c a_u + y s_u a_(u ^ XR), s_u = (-1)^parity(u & zr), y
+// already carrying the sign of the thread's and the tile's Z-type bits; the partner's sign
+// is s_u times (-1)^parity(XR & zr).
+template <int XR>
+__device__ __forceinline__ void reg_pauli_x(double2 (&v)[kE], double c, double2 y, uint32_t zr) {
+    const double sx = (zr & XR) ? -1.0 : 1.0;
+#pragma unroll
+    for (int u = 0; u < kE; ++u) {
+        if (u & XR) continue;
+        const double2 a = v[u], b = v[u ^ XR];
+        const double su = (__popc(static_cast<uint32_t>(u) & zr) & 1u) ? -1.0 : 1.0;
+        const double2 yu = cscale(y, su);
+        v[u] = cmad(yu, b, cscale(a, c));
+        v[u ^ XR] = cmad(cscale(yu, sx), a, cscale(b, c));
+    }
+}
+
+// kRegPauli record: matrices (cos, 0), y, out-of-tile Z-type mask (two exact halves).  A flip
+// set of several register bits reduces to its lowest bit b: with the register permutation
+// U = prod_j CX(b -> b_j) over the other flip bits, U P U has flip bits {b} and Z-type bits
+// zr with b toggled once per b_j among them, so the kernel permutes, rotates on one bit and
+// permutes back (4 + 4 code paths instead of one per flip set, which at 15 unrolled paths
+// made the allocator spill over a kilobyte per thread).
+__device__ __forceinline__ void reg_pauli(double2 (&v)[kE], uint32_t mat, uint32_t xr, uint32_t zr,
+                                          uint32_t zt, uint64_t base) {
+    const double c = lds2(mat).x;
+    double2 y = lds2(mat + 16u);
+    const double2 zd = lds2(mat + 32u);
+    const uint64_t zg = static_cast<uint64_t>(zd.x) | (static_cast<uint64_t>(zd.y) << 32);
+    if ((__popcll(base & zg) + __popc(threadIdx.x & zt)) & 1) y = make_double2(-y.x, -y.y);
+    if (xr == 0) {   // a Z-type string: the diagonal c + y s_u
+        const double2 fp = make_double2(c + y.x, y.y), fm = make_double2(c - y.x, -y.y);
+#pragma unroll
+        for (int u = 0; u < kE; ++u)
+            v[u] = cmul(v[u], (__popc(static_cast<uint32_t>(u) & zr) & 1u) ? fm : fp);
+        return;
+    }
+    const uint32_t b = xr & (0u - xr), rest = xr & ~b;
+    for (uint32_t r = rest; r; r &= r - 1) dispatch_swapx(v, r & (0u - r), b);
+    const uint32_t zr1 = (__popc(zr & rest) & 1u) ? zr ^ b : zr;
+    switch (b) {
+        case 1: reg_pauli_x<1>(v, c, y, zr1); break;
+        case 2: reg_pauli_x<2>(v, c, y, zr1); break;
+        case 4: reg_pauli_x<4>(v, c, y, zr1); break;
+        default: reg_pauli_x<8>(v, c, y, zr1); break;
+    }
+    for (uint32_t r = rest; r; r &= r - 1) dispatch_swapx(v, r & (0u - r), b);
+}
+
 __device__ __forceinline__ uint32_t thread_slot(const RegLayout& ly, uint32_t tbits) {
     uint32_t s = 0;
     for (uint32_t i = 0; i < tbits; ++i)
@@ -337,8 +387,8 @@ __device__ __forceinline__ uint64_t thread_goff(const RegLayout& ly, uint32_t tb
 // pass has dense records on register bits (FP64 FMAs); MMA: it has tensor-path records.  A
 // kernel carries only the paths its pass uses: with both, the register allocation spills
 // (364 bytes at 128 registers against 64 for the FMA path alone and 8 for the tensor path
-// alone), so each pass runs the variant of its own records.
-template <int M, int MINB, bool FMAD, bool MMA>
+// alone), so each pass runs the variant of its own records.  PAULI: it has Pauli rotations.
+template <int M, int MINB, bool FMAD, bool MMA, bool PAULI>
 __global__ void __launch_bounds__(1 << (M - kRegBits), MINB)
 k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
           const RegLayout* __restrict__ layouts, const double2* __restrict__ mats) {
@@ -514,6 +564,10 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                     __syncwarp();
                     reg_mma(v, smat_addr + 16u * moff, op.rcmask);
                 }
+                continue;
+            }
+            if (kind == kRegPauli) {   // rcmask / tcmask: its Z-type bits, not controls
+                if constexpr (PAULI) reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, base);
                 continue;
             }
             if ((threadIdx.x & tc) != tc) continue;
@@ -746,6 +800,10 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
                 reg_mma(v, smat_addr + 16u * moff, op.rcmask);
                 continue;
             }
+            if (kind == kRegPauli) {
+                reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, base);
+                continue;
+            }
             if ((threadIdx.x & tc) != tc) continue;
             const uint32_t rc = op.rcmask;
             const uint32_t mat = kind == kRegDiagDyn ? sdyn_addr + 16u * (dyn_base + op.dyn_off)
@@ -790,11 +848,11 @@ void launch_pipe(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPas
     check_launch("register tile pass (double-buffered)");
 }
 
-template <int M, int MINB, bool FMAD, bool MMA>
+template <int M, int MINB, bool FMAD, bool MMA, bool PAULI>
 void launch_mbf(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
                 const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
     constexpr uint32_t kT = 1u << (M - kRegBits);
-    auto kern = k_regtile<M, MINB, FMAD, MMA>;
+    auto kern = k_regtile<M, MINB, FMAD, MMA, PAULI>;
     cuda_check_launch_attr(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kTileMaxSmem)));
     static const size_t static_smem = [&] {
@@ -813,9 +871,15 @@ void launch_mbf(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass
 template <int M, int MINB>
 void launch_mb(const LaunchCtx& ctx, double2* st, uint32_t batch, const RegPass& p, size_t smem,
                const RegOp* d_ops, const RegLayout* d_layouts, const double2* d_mats) {
-    if (!p.mma_ops) launch_mbf<M, MINB, true, false>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
-    else if (!p.fma_dense) launch_mbf<M, MINB, false, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
-    else launch_mbf<M, MINB, true, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    // four variants: FMA, FMA + Pauli, tensor path, all
+    if (!p.mma_ops) {
+        if (p.pauli_ops) launch_mbf<M, MINB, true, false, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+        else launch_mbf<M, MINB, true, false, false>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    } else if (!p.fma_dense && !p.pauli_ops) {
+        launch_mbf<M, MINB, false, true, false>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    } else {
+        launch_mbf<M, MINB, true, true, true>(ctx, st, batch, p, smem, d_ops, d_layouts, d_mats);
+    }
 }
 
 // Residency per tile size: about 160 registers per thread keep the dense paths free of

@@ -17,7 +17,9 @@ constexpr uint32_t kTileMaxOps = 128;            // operations per pass (staged 
 constexpr uint32_t kTileMaxIters = 32;           // 2^kTileMaxBits / kTileThreads
 constexpr size_t kTileMaxSmem = 200 * 1024;      // tile + staged operation records
 
-enum : uint8_t { kTileDense = 0, kTileDiag = 1, kTilePhase = 2 };
+// kTilePauli: a Pauli rotation exp(-i theta/2 P) inside a register pass (planner only; the
+// shared-memory kernel has no such operation).
+enum : uint8_t { kTileDense = 0, kTileDiag = 1, kTilePhase = 2, kTilePauli = 3 };
 
 // Shared-memory slot of tile element i: the low 3 bits are XOR-ed with a fold of the
 // higher bits so that power-of-two strides spread over the 8 16-byte positions of a
@@ -97,8 +99,15 @@ constexpr uint32_t kRegMaxDynTerms = 48;        // gated phase terms of one per-
 // a set of 8 groups (lanes 2..4) of 4 amplitudes (lanes 0..1), and two k = 4 steps (real
 // parts, then imaginary parts) give every lane its own new amplitude.  Its tile controls are
 // register bits (rcmask) or warp bits (tcmask), never lanes.
+// kRegPauli: exp(-i theta/2 P), a'_i = cos(theta/2) a_i + y (-1)^parity(i & zy) a_(i ^ x) with
+// y = -i sin(theta/2) i^(n_Y) (-1)^parity(x & zy) (kernels::apply_pauli_rotation,
+// src/backend/kernels/gate_kernels.cpp:191-225, x and zy formed as in
+// statevector_simulator.cpp:36-46): its flip bits x are register bits (code = their register
+// mask), its Z-type bits zy are register bits (rcmask), thread bits (tcmask) or out-of-tile
+// qubits (a 64-bit mask among its matrices: (cos, 0), y, then the mask as two exact 32-bit
+// halves).
 enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4,
-                 kRegDiagDyn = 5, kRegMma = 6 };
+                 kRegDiagDyn = 5, kRegMma = 6, kRegPauli = 7 };
 
 struct RegLayout {
     uint16_t rsw[kRegBits];   // tile_swizzle(1 << rpos[i])
@@ -143,6 +152,7 @@ struct RegPass {
                               // other barrier provides it (relabelled stores, in place)
     uint32_t fma_dense;       // some record is a dense op on register bits (kRegDense)
     uint32_t mma_ops;         // some record is a tensor-path block (kRegMma)
+    uint32_t pauli_ops;       // some record is a Pauli rotation (kRegPauli)
 };
 
 static_assert(sizeof(RegLayout) % 4 == 0 && sizeof(RegOp) == 32, "staged as 32-bit words");

@@ -40,6 +40,7 @@ TileConfig default_tile_config(uint32_t n) {
     c.reg = env_int("LQCS_TILE_REG", 1) != 0;
     c.search = env_int("LQCS_TILE_SEARCH", 1) != 0;
     c.mma = env_int("LQCS_REG_MMA", 0) != 0;
+    c.pauli = env_int("LQCS_TILE_PAULI", 1) != 0;
     c.m = std::max<uint32_t>(kTileMinBits, std::min<uint32_t>(std::min<uint32_t>(c.m, kTileMaxBits), n));
     c.L = std::min<uint32_t>(std::min(c.L, c.m), kTileMinBits);   // column bits come from the thread index
     if (c.m - c.L > kTileMaxHigh) c.L = c.m - kTileMaxHigh;
@@ -47,9 +48,26 @@ TileConfig default_tile_config(uint32_t n) {
     return c;
 }
 
-// Qubits a gate needs inside the tile, or false if it cannot run in a tile at all.
+bool native_pauli(const GateDesc& g, const TileConfig& cfg) {
+    if (!cfg.reg || !cfg.pauli || g.type != LQCS_GATE_PAULI_ROTATION || g.n_controls != 0 || g.slot)
+        return false;
+    uint32_t flips = 0;
+    for (char ch : g.pauli) flips += ch == 'X' || ch == 'Y';
+    return flips <= kRegBits;
+}
+
+// Qubits a gate needs inside the tile, or false if it cannot run in a tile at all.  A native
+// Pauli rotation needs only its X/Y qubits there (its Z-type qubits act through parities).
 static bool tile_requirements(const GateDesc& g, const TileConfig& c, std::vector<uint32_t>& need) {
     need.clear();
+    if (native_pauli(g, c)) {
+        const uint32_t k = g.base_qubits();
+        for (uint32_t j = 0; j < k; ++j) {
+            const char ch = g.pauli[k - 1 - j];   // local bit j <-> pauli[k-1-j] (Gate::pauli_masks)
+            if (ch == 'X' || ch == 'Y') need.push_back(g.targets()[j]);
+        }
+        return true;
+    }
     if (is_phase_gate(g)) return g.qubits.size() <= 8;   // at most 8 local phase bits
     const uint32_t k = g.base_qubits();
     if (k == 0 || k > kTileMaxK) return false;
@@ -305,6 +323,7 @@ bool is_x(const std::vector<cd>& m) {
 }  // namespace
 
 double local_op_flops(const LocalOp& o, bool x_free) {
+    if (o.kind == kTilePauli) return o.lt.empty() ? 6.0 : 16.0;   // op_flops_per_amp of PAULI
     const double frac = std::ldexp(1.0, -(__builtin_popcount(o.lmask) + __builtin_popcountll(o.gcmask)));
     if (o.kind != kTileDense) return 6.0 * frac;
     if (x_free && !o.variant && o.lt.size() == 1 && o.sel.empty() && is_x(o.m)) return 0.0;
@@ -479,7 +498,7 @@ static void merge_diagonal_runs(std::vector<LocalOp>& ops, uint32_t max_bits, bo
                 }
             }
             // q stays: later diagonal work may pass it only on bits it does not target
-            if (q.kind == kTileDense)
+            if (q.kind == kTileDense || q.kind == kTilePauli)
                 for (uint32_t b : q.lt) blocked |= 1u << b;
         }
         if (!merged) continue;   // a lone op keeps its own (cheaper) form
@@ -523,7 +542,8 @@ static void fold_single_qubit_ops(std::vector<LocalOp>& ops, uint32_t max_select
             as_diag.m = {cd{1, 0}, ops[i].m[0]};
         }
         const LocalOp& p = one_bit_phase ? as_diag : ops[i];
-        if (p.kind == kTilePhase || p.lt.size() != 1 || p.lmask || p.gcmask || !p.dyn.empty())
+        if (p.kind == kTilePhase || p.kind == kTilePauli || p.lt.size() != 1 || p.lmask ||
+            p.gcmask || !p.dyn.empty())
             continue;
         const uint32_t a = p.lt[0];
         for (size_t j = i + 1; j < ops.size(); ++j) {
@@ -581,7 +601,7 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
                                     const TileConfig& cfg, uint32_t max_select,
                                     const std::vector<std::array<cd, 4>>* slot_mats,
                                     uint32_t max_diag, bool dyn_terms,
-                                    std::vector<uint32_t>* store_qubits) {
+                                    std::vector<uint32_t>* store_qubits, bool native_rotations) {
     LocalMap lm{cfg.L, item.hbits, {}};
     std::vector<LocalOp> out;
     // a noise slot takes this state's matrix (identity when no table is given)
@@ -705,6 +725,38 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
 
     for (uint32_t gi : item.gates) {
         const GateDesc& g = gates[gi];
+        // a native Pauli rotation: closes the blocks on its tile qubits and runs on its own
+        if (native_rotations && native_pauli(g, cfg)) {
+            for (uint32_t q : g.qubits)
+                if (lm.local(q) >= 0 && owner[q] >= 0) emit_block(open[owner[q]]);
+            const PauliMasks pm = pauli_local_masks(g.pauli);
+            LocalOp op;
+            op.kind = kTilePauli;
+            uint64_t xg = 0, zg = 0;
+            for (uint32_t j = 0; j < g.base_qubits(); ++j) {
+                const uint32_t q = g.targets()[j];
+                const int l = lm.local(q);
+                if ((pm.x >> j) & 1) {
+                    if (l < 0) logic("tile lowering: a Pauli rotation flips a qubit outside the tile");
+                    op.lt.push_back(static_cast<uint32_t>(l));
+                    xg |= uint64_t{1} << q;
+                }
+                if ((pm.zy >> j) & 1) {
+                    zg |= uint64_t{1} << q;
+                    if (l >= 0) op.lmask |= 1u << l;
+                    else op.pz_out |= uint64_t{1} << q;
+                }
+            }
+            std::sort(op.lt.begin(), op.lt.end());
+            // y = (-i sin) i^n_Y, as apply_pauli_rotation forms it, times (-1)^parity(x & zy)
+            const double h = g.params.at(0) / 2;
+            static const cd kIPow[4] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+            cd y = cd{0.0, -std::sin(h)} * kIPow[pm.n_y % 4];
+            if (__builtin_popcountll(xg & zg) & 1) y = -y;
+            op.m = {cd{std::cos(h), 0.0}, y};
+            out.push_back(std::move(op));
+            continue;
+        }
         // a SWAP of two tile qubits moves no data: the two tile bits trade qubits for the rest
         // of the pass, and the store writes each tile bit to its qubit's place
         if (store_qubits && g.type == LQCS_GATE_SWAP && g.n_controls == 0 && !g.slot &&
@@ -837,7 +889,7 @@ struct Use {
 };
 Use op_use(const LocalOp& o) {
     Use u;
-    if (o.kind == kTileDense) u.nd = target_mask(o);
+    if (o.kind == kTileDense || o.kind == kTilePauli) u.nd = target_mask(o);
     else if (o.kind == kTileDiag) u.dg = target_mask(o);
     u.dg |= o.lmask;
     return u;
@@ -854,6 +906,7 @@ struct Lay {
 // of a warp takes part in the instruction); any other dense op needs its targets on
 // register bits.
 bool fits(const LocalOp& o, bool mma, const Lay& ly) {
+    if (o.kind == kTilePauli) return (target_mask(o) & ~ly.S) == 0;   // flips on register bits
     if (o.kind != kTileDense) return true;
     if (mma) return ly.P != 0 && (target_mask(o) & ~ly.P) == 0 && (o.lmask & ~(ly.S | ly.W)) == 0;
     return (target_mask(o) & ~ly.S) == 0;
@@ -890,7 +943,9 @@ size_t covered(const std::vector<LocalOp>& ops, const std::vector<uint8_t>& mma,
                const std::vector<uint32_t>& pending, uint32_t S) {
     size_t c = 0;
     for (uint32_t i : pending)
-        if (ops[i].kind == kTileDense && !mma[i] && (target_mask(ops[i]) & ~S) == 0) ++c;
+        if ((ops[i].kind == kTileDense || ops[i].kind == kTilePauli) && !mma[i] &&
+            (target_mask(ops[i]) & ~S) == 0)
+            ++c;
     return c;
 }
 
@@ -963,7 +1018,7 @@ uint32_t pick_warp_bits(const std::vector<LocalOp>& ops, const std::vector<uint3
                         uint32_t avail, uint32_t count, uint32_t pair = 0) {
     uint32_t usage[32] = {};
     for (uint32_t i : pending)
-        if (ops[i].kind == kTileDense)
+        if (ops[i].kind == kTileDense || ops[i].kind == kTilePauli)
             for (uint32_t b : ops[i].lt) ++usage[b];
     uint32_t W = 0;
     for (uint32_t k = 0; k < count; ++k) {
@@ -1058,6 +1113,12 @@ void append_matrices(const LocalOp& o, const RegLayout& ly, uint32_t S, std::vec
         }
         return;
     }
+    if (o.kind == kTilePauli) {   // (cos, 0), y, the out-of-tile Z-type qubits as two halves
+        mats.insert(mats.end(), o.m.begin(), o.m.end());
+        mats.emplace_back(static_cast<double>(o.pz_out & 0xffffffffu),
+                          static_cast<double>(o.pz_out >> 32));
+        return;
+    }
     if (o.kind == kTilePhase || o.kind == kTileDiag) {
         mats.insert(mats.end(), o.m.begin(), o.m.end());
         // per-tile terms: the factor, then {gcmask low 32 bits, gcmask high 32 bits * 64 +
@@ -1124,6 +1185,10 @@ RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m,
             logic("register tile lowering: a tensor-path block is controlled by a lane bit");
         r.kind = kRegMma;
         r.k = 2;   // always a 4 x 4 block (a one-target op with the identity on the other lane)
+    } else if (o.kind == kTilePauli) {   // Z-type tile bits went to rcmask / tcmask above
+        r.kind = kRegPauli;
+        r.k = 0;
+        for (uint32_t b : o.lt) r.code = static_cast<uint8_t>(r.code | (1u << ridx[b]));
     } else if (o.kind == kTilePhase) {
         r.kind = kRegPhase;
     } else if (o.kind == kTileDiag) {
@@ -1158,7 +1223,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
         state_slots && !state_slots->empty() ? &(*state_slots)[0] : nullptr;
     std::vector<uint32_t> store_q;
     const std::vector<LocalOp> ops =
-        pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true, &store_q);
+        pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true, &store_q, true);
     for (const LocalOp& o : ops)
         if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : kRegMaxDiag))
             return false;
@@ -1321,7 +1386,7 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
             std::vector<uint32_t> store_b;
             const std::vector<LocalOp> ob = pass_local_ops(item, gates, cfg, max_select,
                                                            &(*state_slots)[b], kRegMaxDiag, true,
-                                                           &store_b);
+                                                           &store_b, true);
             if (ob.size() != ops.size() || store_b != store_q) return false;
             for (size_t i = 0; i < ops.size(); ++i)
                 if (!same_shape(ops[i], ob[i])) return false;
@@ -1365,10 +1430,11 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     // the per-tile table barrier, both after the loads, order them; otherwise the kernel
     // adds a barrier after the loads.
     pass.load_barrier = pass.relabel && !sync_tiles && dyn_rec.empty() ? 1u : 0u;
-    pass.fma_dense = pass.mma_ops = 0;
+    pass.fma_dense = pass.mma_ops = pass.pauli_ops = 0;
     for (const RegOp& r : rec) {
         if (r.kind == kRegDense) pass.fma_dense = 1;
         if (r.kind == kRegMma) pass.mma_ops = 1;
+        if (r.kind == kRegPauli) pass.pauli_ops = 1;
     }
     for (size_t d = 0; d < dyn_rec.size(); ++d) pass.dyn_rec[d] = static_cast<uint8_t>(dyn_rec[d]);
     ops_out.insert(ops_out.end(), rec.begin(), rec.end());

@@ -17,7 +17,15 @@ struct TileConfig {
     bool mma = false;      // register passes: one- and two-qubit blocks on the FP64 tensor
                            // path (mma.sync m8n8k4) instead of FP64 FMAs over register bits
                            // (LQCS_REG_MMA=1)
+    bool pauli = true;     // register passes: Pauli rotations whose X/Y qubits (at most
+                           // kRegBits) are tile qubits run inside the pass (LQCS_TILE_PAULI=0:
+                           // only those of at most kTileMaxK qubits, as dense blocks)
 };
+
+// Whether gate g runs as a native Pauli rotation inside a register pass (cfg.reg, cfg.pauli,
+// an uncontrolled rotation with at most kRegBits X/Y qubits; its Z qubits need not be in the
+// tile).  A pass holding one that does not fit the register kernel is split at it.
+bool native_pauli(const GateDesc& g, const TileConfig& cfg);
 TileConfig default_tile_config(uint32_t n);
 
 // A pass (hbits + gates applied in program order) or one gate run on its own.
@@ -51,6 +59,9 @@ struct LocalOp {
     std::vector<cd> m;              // dense: 2^k x 2^k, diagonal: 2^k, phase: the factor;
                                     // with sel, one such block per selector value
     std::vector<DynTerm> dyn;       // diagonal: gated phase terms multiplied into m per tile
+    // kTilePauli: lt = the flip (X/Y) bits, lmask = the Z-type (Z/Y) tile bits, pz_out = the
+    // Z-type qubits outside the tile, m = {(cos, 0), y} (see kRegPauli)
+    uint64_t pz_out = 0;
 };
 
 // The operations of one pass in program order, neighbouring gates fused into blocks of at
@@ -65,7 +76,8 @@ std::vector<LocalOp> pass_local_ops(const PlanItem& item, const std::vector<Gate
                                     const TileConfig& cfg, uint32_t max_select,
                                     const std::vector<std::array<cd, 4>>* slot_mats = nullptr,
                                     uint32_t max_diag = kTileMaxK, bool dyn_terms = false,
-                                    std::vector<uint32_t>* store_qubits = nullptr);
+                                    std::vector<uint32_t>* store_qubits = nullptr,
+                                    bool native_rotations = false);
 
 // Append the tile operations of one pass to ops_out (matrices to arena) and fill `pass`.
 void lower_pass(const PlanItem& item, const std::vector<GateDesc>& gates, const TileConfig& cfg,

@@ -286,3 +286,66 @@ def test_register_passes_on_the_tensor_path(port, ref, tile_env, m):
     init = W.gaussian_state(16, seed=5)
     q = lq.algorithms.qft(16)
     assert np.max(np.abs(run(q, TILE, init) - ref.evolve_from(q, init))) < TOL
+
+
+def _pauli_circuit(n, n_gates, seed):
+    rng = np.random.default_rng(seed)
+    qc = lq.QuantumCircuit(n)
+    for _ in range(n_gates):
+        r = float(rng.uniform())
+        q = [int(x) for x in rng.permutation(n)]
+        if r < 0.4:
+            qc.u(*(float(x) for x in rng.uniform(0, 2 * np.pi, 3)), q[0])
+        elif r < 0.55:
+            qc.cx(q[0], q[1])
+        elif r < 0.6:
+            qc.cp(float(rng.uniform(0, 6.3)), q[0], q[1])
+        else:
+            w = int(rng.integers(1, min(9, n + 1)))
+            qc.rp(float(rng.uniform(-np.pi, np.pi)),
+                  "".join("XYZ"[int(rng.integers(3))] for _ in range(w)), q[:w])
+    return qc
+
+
+@pytest.fixture
+def pauli_env():
+    saved = os.environ.get("LQCS_TILE_PAULI")
+    yield lambda v: os.environ.__setitem__("LQCS_TILE_PAULI", str(v))
+    if saved is None:
+        os.environ.pop("LQCS_TILE_PAULI", None)
+    else:
+        os.environ["LQCS_TILE_PAULI"] = saved
+
+
+@pytest.mark.parametrize("n", [13, 16, 20])
+@pytest.mark.parametrize("cfg", [(12, 5, 2, 1, 0), (11, 5, 2, 1, 0), (12, 5, 2, 1, 1), (12, 5, 4, 1, 0)],
+                         ids=["m12", "m11", "m12_tensor", "inner4_split"])
+def test_native_pauli_rotations_in_register_passes(port, tile_env, pauli_env, n, cfg):
+    """Pauli rotations of weight 1..8 whose X/Y qubits (at most four) are tile qubits run
+    inside register passes — Z qubits inside or outside the tile act through parities; the
+    others run on their own.  inner4_split: 4-qubit blocks keep passes off the register
+    kernel, so the shared-memory passes split at each rotation.  Both against the oracle and
+    against LQCS_TILE_PAULI=0 (rotations of at most four qubits as dense blocks)."""
+    tile_env(*cfg)
+    init = W.gaussian_state(n, seed=n + 1)
+    qc = _pauli_circuit(n, 160, seed=3 * n + cfg[0])
+    want = port.run_statevector(qc, fuse=False, state=init)
+    pauli_env(1)
+    got = run(qc, TILE, init)
+    assert np.max(np.abs(got - want)) < TOL
+    if cfg[2] <= 3:
+        assert 7 in kernel_kinds(qc)
+    pauli_env(0)
+    assert np.max(np.abs(run(qc, TILE, init) - want)) < TOL
+
+
+def test_random_mix_24q_native_rotations_equal_gate_by_gate():
+    """The cost-model workload's gate mix (10 % Pauli rotations of weight 2..8) at 24 qubits,
+    default path, against gate-by-gate application on the device."""
+    qc = W.random_mix_circuit(24, 12, seed=5)
+    init = W.gaussian_state(24, seed=24)
+    a = lq.Statevector.from_numpy(init)
+    lq.simulator.CompiledCircuit(qc, True, 0, 0).apply(a)
+    b = lq.Statevector.from_numpy(init)
+    lq.simulator.CompiledCircuit(qc, True, 0, 3).apply(b)
+    assert float(np.max(np.abs(a.to_numpy() - b.to_numpy()))) < TOL

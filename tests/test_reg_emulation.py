@@ -77,6 +77,28 @@ def tile_circuit(n, n_gates, seed):
     return qc
 
 
+def pauli_circuit(n, n_gates, seed):
+    """U3, CX and Pauli rotations of weight 2..8 on random qubits (X/Y/Z uniform, at most
+    four X/Y — more run as passes of their own, which this emulation does not take)."""
+    rng = np.random.default_rng(seed)
+    qc = lq.QuantumCircuit(n)
+    for _ in range(n_gates):
+        r = float(rng.uniform())
+        q = [int(x) for x in rng.permutation(n)]
+        if r < 0.4:
+            qc.u(*(float(x) for x in rng.uniform(0, 2 * np.pi, 3)), q[0])
+        elif r < 0.6:
+            qc.cx(q[0], q[1])
+        else:
+            w = int(rng.integers(2, 9))
+            chars = ["XYZ"[int(rng.integers(3))] for _ in range(w)]
+            flips = [i for i, ch in enumerate(chars) if ch != "Z"]
+            for i in flips[4:]:
+                chars[i] = "Z"
+            qc.rp(float(rng.uniform(-np.pi, np.pi)), "".join(chars), q[:w])
+    return qc
+
+
 def circuits():
     yield "brickwork14", W.brickwork(14, 8, seed=3)
     yield "brickwork17", W.brickwork(17, 6, seed=4)
@@ -86,6 +108,8 @@ def circuits():
     yield "qft15", lq.algorithms.qft(15)
     yield "random13", tile_circuit(13, 150, seed=5)
     yield "random16", tile_circuit(16, 200, seed=6)
+    yield "pauli14", pauli_circuit(14, 120, seed=7)
+    yield "pauli18", pauli_circuit(18, 150, seed=8)
 
 
 @pytest.mark.parametrize("mma", ["1", "0"], ids=["tensor_path", "fma_path"])
