@@ -333,8 +333,12 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
             uint32_t o = 0;
             while (o <= p.n_ops) {
                 uint32_t end = o;
-                while (end < p.n_ops && !((ops[end].kind == kRegRemap || ops[end].kind == kRegMma) &&
-                                          (base & ops[end].gcmask) == ops[end].gcmask))
+                auto warp_wide = [&](const RegOp& r) {
+                    return r.kind == kRegRemap || r.kind == kRegMma ||
+                           (r.kind == kRegPauli && r.loc[0] != 0);
+                };
+                while (end < p.n_ops &&
+                       !(warp_wide(ops[end]) && (base & ops[end].gcmask) == ops[end].gcmask))
                     ++end;
                 // [o, end): non-remap operations, each thread independently
                 for (uint32_t t = 0; t < kT; ++t) {
@@ -437,6 +441,31 @@ void emulate_reg_pass(const RegPass& pass, const RegOp* ops, const RegLayout* la
                     }
                 }
                 if (end >= p.n_ops) break;
+                if (ops[end].kind == kRegPauli) {
+                    // flips on lanes: a lane reads its partner lane's registers (shuffles), so
+                    // the warp's values are read before any is written
+                    const RegOp& op = ops[end];
+                    if (in) {
+                        const std::vector<cd> snap = v;
+                        const cd c = mats[op.mat_off];
+                        const cd y0 = mats[op.mat_off + 1];
+                        const cd zd = mats[op.mat_off + 2];
+                        const uint64_t zg = static_cast<uint64_t>(zd.real()) |
+                                            (static_cast<uint64_t>(zd.imag()) << 32);
+                        for (uint32_t t = 0; t < kT; ++t) {
+                            const uint32_t tp = t ^ op.loc[0];
+                            for (uint32_t u = 0; u < kE; ++u) {
+                                const int par = __builtin_popcountll(base & zg) +
+                                                __builtin_popcount(t & op.tcmask) +
+                                                __builtin_popcount(u & op.rcmask);
+                                const cd y = (par & 1) ? -y0 : y0;
+                                v[t * kE + u] = c * snap[t * kE + u] + y * snap[tp * kE + (u ^ op.code)];
+                            }
+                        }
+                    }
+                    o = end + 1;
+                    continue;
+                }
                 if (ops[end].kind == kRegMma) {
                     // every lane of a warp whose warp-bit controls are all 1 (lane controls
                     // never occur: the lowering refuses them); register u's quad of lanes

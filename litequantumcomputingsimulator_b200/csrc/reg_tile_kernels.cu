@@ -336,6 +336,32 @@ __device__ __forceinline__ void reg_pauli_x(double2 (&v)[kE], double c, double2 
     }
 }
 
+// The same with flips on lanes too (lane mask xl): the partner of (u, lane) is (u ^ XR,
+// lane ^ xl), fetched by shuffle; XR = 0: flips on lanes only.  Every lane of the warp runs it.
+template <int XR>
+__device__ __forceinline__ void reg_pauli_xl(double2 (&v)[kE], double c, double2 y, uint32_t zr,
+                                             uint32_t xl) {
+    const int m = static_cast<int>(xl);
+    if constexpr (XR == 0) {
+#pragma unroll
+        for (int u = 0; u < kE; ++u) {
+            const double2 b = shfl_xor_d2(v[u], m);
+            const double su = (__popc(static_cast<uint32_t>(u) & zr) & 1u) ? -1.0 : 1.0;
+            v[u] = cmad(cscale(y, su), b, cscale(v[u], c));
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kE; ++u) {
+            if (u & XR) continue;
+            const double2 pu = shfl_xor_d2(v[u ^ XR], m), pw = shfl_xor_d2(v[u], m);
+            const double su = (__popc(static_cast<uint32_t>(u) & zr) & 1u) ? -1.0 : 1.0;
+            const double sw = (__popc(static_cast<uint32_t>(u ^ XR) & zr) & 1u) ? -1.0 : 1.0;
+            v[u] = cmad(cscale(y, su), pu, cscale(v[u], c));
+            v[u ^ XR] = cmad(cscale(y, sw), pw, cscale(v[u ^ XR], c));
+        }
+    }
+}
+
 // kRegPauli record: matrices (cos, 0), y, out-of-tile Z-type mask (two exact halves).  A flip
 // set of several register bits reduces to its lowest bit b: with the register permutation
 // U = prod_j CX(b -> b_j) over the other flip bits, U P U has flip bits {b} and Z-type bits
@@ -343,12 +369,16 @@ __device__ __forceinline__ void reg_pauli_x(double2 (&v)[kE], double c, double2 
 // permutes back (4 + 4 code paths instead of one per flip set, which at 15 unrolled paths
 // made the allocator spill over a kilobyte per thread).
 __device__ __forceinline__ void reg_pauli(double2 (&v)[kE], uint32_t mat, uint32_t xr, uint32_t zr,
-                                          uint32_t zt, uint64_t base) {
+                                          uint32_t zt, uint32_t xl, uint64_t base) {
     const double c = lds2(mat).x;
     double2 y = lds2(mat + 16u);
     const double2 zd = lds2(mat + 32u);
     const uint64_t zg = static_cast<uint64_t>(zd.x) | (static_cast<uint64_t>(zd.y) << 32);
     if ((__popcll(base & zg) + __popc(threadIdx.x & zt)) & 1) y = make_double2(-y.x, -y.y);
+    if (xl != 0 && xr == 0) {   // flips on lanes only
+        reg_pauli_xl<0>(v, c, y, zr, xl);
+        return;
+    }
     if (xr == 0) {   // a Z-type string: the diagonal c + y s_u
         const double2 fp = make_double2(c + y.x, y.y), fm = make_double2(c - y.x, -y.y);
 #pragma unroll
@@ -359,11 +389,20 @@ __device__ __forceinline__ void reg_pauli(double2 (&v)[kE], uint32_t mat, uint32
     const uint32_t b = xr & (0u - xr), rest = xr & ~b;
     for (uint32_t r = rest; r; r &= r - 1) dispatch_swapx(v, r & (0u - r), b);
     const uint32_t zr1 = (__popc(zr & rest) & 1u) ? zr ^ b : zr;
-    switch (b) {
-        case 1: reg_pauli_x<1>(v, c, y, zr1); break;
-        case 2: reg_pauli_x<2>(v, c, y, zr1); break;
-        case 4: reg_pauli_x<4>(v, c, y, zr1); break;
-        default: reg_pauli_x<8>(v, c, y, zr1); break;
+    if (xl != 0) {
+        switch (b) {
+            case 1: reg_pauli_xl<1>(v, c, y, zr1, xl); break;
+            case 2: reg_pauli_xl<2>(v, c, y, zr1, xl); break;
+            case 4: reg_pauli_xl<4>(v, c, y, zr1, xl); break;
+            default: reg_pauli_xl<8>(v, c, y, zr1, xl); break;
+        }
+    } else {
+        switch (b) {
+            case 1: reg_pauli_x<1>(v, c, y, zr1); break;
+            case 2: reg_pauli_x<2>(v, c, y, zr1); break;
+            case 4: reg_pauli_x<4>(v, c, y, zr1); break;
+            default: reg_pauli_x<8>(v, c, y, zr1); break;
+        }
     }
     for (uint32_t r = rest; r; r &= r - 1) dispatch_swapx(v, r & (0u - r), b);
 }
@@ -567,7 +606,8 @@ k_regtile(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ ops,
                 continue;
             }
             if (kind == kRegPauli) {   // rcmask / tcmask: its Z-type bits, not controls
-                if constexpr (PAULI) reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, base);
+                if constexpr (PAULI)
+                    reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, op.loc[0], base);
                 continue;
             }
             if ((threadIdx.x & tc) != tc) continue;
@@ -801,7 +841,7 @@ k_regtile_pipe(double2* __restrict__ st, RegPass p, const RegOp* __restrict__ op
                 continue;
             }
             if (kind == kRegPauli) {
-                reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, base);
+                reg_pauli(v, smat_addr + 16u * moff, op.code, op.rcmask, tc, op.loc[0], base);
                 continue;
             }
             if ((threadIdx.x & tc) != tc) continue;

@@ -89,6 +89,8 @@ constexpr uint32_t kRegMaxDiag = 6;             // widest diagonal operation (64
 constexpr uint32_t kRegMaxDyn = 8;              // per-tile diagonals per pass
 constexpr uint32_t kRegMaxDynEntries = 512;     // their table entries per pass
 constexpr uint32_t kRegMaxDynTerms = 48;        // gated phase terms of one per-tile diagonal
+constexpr uint32_t kRegPauliMaxFlips = 9;       // X/Y qubits of a Pauli rotation in a pass:
+                                                // register bits and lanes
 
 // kRegDiagDyn: a diagonal whose table is built at the start of every tile from a base table
 // and gated phase terms (the matrices hold the 2^k base entries, then per term its factor and
@@ -103,9 +105,9 @@ constexpr uint32_t kRegMaxDynTerms = 48;        // gated phase terms of one per-
 // y = -i sin(theta/2) i^(n_Y) (-1)^parity(x & zy) (kernels::apply_pauli_rotation,
 // src/backend/kernels/gate_kernels.cpp:191-225, x and zy formed as in
 // statevector_simulator.cpp:36-46): its flip bits x are register bits (code = their register
-// mask), its Z-type bits zy are register bits (rcmask), thread bits (tcmask) or out-of-tile
-// qubits (a 64-bit mask among its matrices: (cos, 0), y, then the mask as two exact 32-bit
-// halves).
+// mask) or lanes (loc[0] = their lane mask: the partner comes by shuffle), its Z-type bits zy
+// are register bits (rcmask), thread bits (tcmask) or out-of-tile qubits (a 64-bit mask among
+// its matrices: (cos, 0), y, then the mask as two exact 32-bit halves).
 enum : uint8_t { kRegDense = 0, kRegDiag = 1, kRegPhase = 2, kRegSwapX = 3, kRegRemap = 4,
                  kRegDiagDyn = 5, kRegMma = 6, kRegPauli = 7 };
 

@@ -53,7 +53,7 @@ bool native_pauli(const GateDesc& g, const TileConfig& cfg) {
         return false;
     uint32_t flips = 0;
     for (char ch : g.pauli) flips += ch == 'X' || ch == 'Y';
-    return flips <= kRegBits;
+    return flips <= kRegPauliMaxFlips;
 }
 
 // Qubits a gate needs inside the tile, or false if it cannot run in a tile at all.  A native
@@ -906,7 +906,7 @@ struct Lay {
 // of a warp takes part in the instruction); any other dense op needs its targets on
 // register bits.
 bool fits(const LocalOp& o, bool mma, const Lay& ly) {
-    if (o.kind == kTilePauli) return (target_mask(o) & ~ly.S) == 0;   // flips on register bits
+    if (o.kind == kTilePauli) return (target_mask(o) & ly.W) == 0;   // flips on registers, lanes
     if (o.kind != kTileDense) return true;
     if (mma) return ly.P != 0 && (target_mask(o) & ~ly.P) == 0 && (o.lmask & ~(ly.S | ly.W)) == 0;
     return (target_mask(o) & ~ly.S) == 0;
@@ -1188,7 +1188,15 @@ RegOp make_record(const LocalOp& o, const RegLayout& ly, uint32_t S, uint32_t m,
     } else if (o.kind == kTilePauli) {   // Z-type tile bits went to rcmask / tcmask above
         r.kind = kRegPauli;
         r.k = 0;
-        for (uint32_t b : o.lt) r.code = static_cast<uint8_t>(r.code | (1u << ridx[b]));
+        for (uint32_t b : o.lt) {
+            if ((S >> b) & 1) {
+                r.code = static_cast<uint8_t>(r.code | (1u << ridx[b]));
+            } else {
+                if (tidx[b] >= static_cast<int>(kLaneBits))
+                    logic("register tile lowering: a Pauli rotation flips a warp bit");
+                r.loc[0] = static_cast<uint8_t>(r.loc[0] | (1u << tidx[b]));
+            }
+        }
     } else if (o.kind == kTilePhase) {
         r.kind = kRegPhase;
     } else if (o.kind == kTileDiag) {
@@ -1225,7 +1233,8 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
     const std::vector<LocalOp> ops =
         pass_local_ops(item, gates, cfg, max_select, slots0, kRegMaxDiag, true, &store_q, true);
     for (const LocalOp& o : ops)
-        if (o.kind != kTilePhase && o.lt.size() > (o.kind == kTileDense ? kRegMaxK : kRegMaxDiag))
+        if (o.kind != kTilePhase && o.kind != kTilePauli &&
+            o.lt.size() > (o.kind == kTileDense ? kRegMaxK : kRegMaxDiag))
             return false;
     std::vector<Use> use;
     for (const LocalOp& o : ops) use.push_back(op_use(o));
@@ -1313,6 +1322,15 @@ bool lower_pass_reg_sel(const PlanItem& item, const std::vector<GateDesc>& gates
                 seq.emplace_back(-2, cur);
                 sync_tiles = true;
             }
+            continue;
+        }
+        if (f.kind == kTilePauli) {   // its flips on warp bits: new warp bits outside them
+            W = pick_warp_bits(ops, pending, all & ~target_mask(f), nwarp);
+            S = choose_set(ops, use, mma, pending, 0, all & ~W, m, all & ~W, 0, W);
+            P = next_pair(all & ~W & ~S);
+            cur = layout_index(S, W, P);
+            seq.emplace_back(-2, cur);
+            sync_tiles = true;
             continue;
         }
         const uint32_t must = target_mask(f);

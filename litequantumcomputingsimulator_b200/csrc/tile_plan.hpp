@@ -18,13 +18,15 @@ struct TileConfig {
                            // path (mma.sync m8n8k4) instead of FP64 FMAs over register bits
                            // (LQCS_REG_MMA=1)
     bool pauli = true;     // register passes: Pauli rotations whose X/Y qubits (at most
-                           // kRegBits) are tile qubits run inside the pass (LQCS_TILE_PAULI=0:
-                           // only those of at most kTileMaxK qubits, as dense blocks)
+                           // kRegPauliMaxFlips) are tile qubits run inside the pass
+                           // (LQCS_TILE_PAULI=0: only those of at most kTileMaxK qubits, as
+                           // dense blocks)
 };
 
 // Whether gate g runs as a native Pauli rotation inside a register pass (cfg.reg, cfg.pauli,
-// an uncontrolled rotation with at most kRegBits X/Y qubits; its Z qubits need not be in the
-// tile).  A pass holding one that does not fit the register kernel is split at it.
+// an uncontrolled rotation with at most kRegPauliMaxFlips X/Y qubits — on register bits and
+// lanes; its Z qubits need not be in the tile).  A pass holding one that does not fit the
+// register kernel is split at it.
 bool native_pauli(const GateDesc& g, const TileConfig& cfg);
 TileConfig default_tile_config(uint32_t n);
 

@@ -77,9 +77,9 @@ def tile_circuit(n, n_gates, seed):
     return qc
 
 
-def pauli_circuit(n, n_gates, seed):
+def pauli_circuit(n, n_gates, seed, max_flips=4):
     """U3, CX and Pauli rotations of weight 2..8 on random qubits (X/Y/Z uniform, at most
-    four X/Y — more run as passes of their own, which this emulation does not take)."""
+    max_flips X/Y)."""
     rng = np.random.default_rng(seed)
     qc = lq.QuantumCircuit(n)
     for _ in range(n_gates):
@@ -93,7 +93,7 @@ def pauli_circuit(n, n_gates, seed):
             w = int(rng.integers(2, 9))
             chars = ["XYZ"[int(rng.integers(3))] for _ in range(w)]
             flips = [i for i, ch in enumerate(chars) if ch != "Z"]
-            for i in flips[4:]:
+            for i in flips[max_flips:]:
                 chars[i] = "Z"
             qc.rp(float(rng.uniform(-np.pi, np.pi)), "".join(chars), q[:w])
     return qc
@@ -110,6 +110,7 @@ def circuits():
     yield "random16", tile_circuit(16, 200, seed=6)
     yield "pauli14", pauli_circuit(14, 120, seed=7)
     yield "pauli18", pauli_circuit(18, 150, seed=8)
+    yield "pauli16_lanes", pauli_circuit(16, 150, seed=9, max_flips=8)
 
 
 @pytest.mark.parametrize("mma", ["1", "0"], ids=["tensor_path", "fma_path"])
