@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--seed", type=int, default=2025)
+    ap.add_argument("--workload", choices=["brickwork", "random_mix"], default="brickwork",
+                    help="timed circuit: the headline brickwork, or the cost-model gate mix "
+                         "(50 %% U3, 30 %% CX/CZ, 10 %% RZZ, 10 %% Pauli rotations of weight "
+                         "2..8) for profiling; the CPU baseline covers the brickwork only")
     ap.add_argument("--fusion-width", type=int, default=0)
     ap.add_argument("--fusion-mode", type=int, default=0)
     ap.add_argument("--no-extras", action="store_true", help="skip sweep/QFT/adjoint/CPU legs")
@@ -364,7 +368,10 @@ def main():
     from litequantumcomputingsimulator_b200 import workloads as W
 
     n, depth = args.qubits, args.depth
-    qc = W.brickwork(n, depth, args.seed)
+    if args.workload == "random_mix":
+        qc = W.random_mix_circuit(n, depth, args.seed)
+    else:
+        qc = W.brickwork(n, depth, args.seed)
     gate_bytes = W.alg_bytes(qc)
     n_gates = qc.num_instructions()
     hbm_peak, peak_kind = peaks()
@@ -455,7 +462,7 @@ def main():
         sharded = run_sharded(lq, W, dist, device, world)
 
     cpu = None
-    if rank == 0 and not args.no_cpu and world == 1:
+    if rank == 0 and not args.no_cpu and world == 1 and args.workload == "brickwork":
         try:
             cpu = cpu_baseline(n, qc, depth, args.seed)
         except Exception as e:  # noqa: BLE001
@@ -466,8 +473,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic (seeded brickwork circuit, random-init |0> state)",
-            "config": {"workload": f"brickwork n={n} depth={depth} seed={args.seed} "
+            "data": f"synthetic (seeded {args.workload} circuit, |0> initial state)",
+            "config": {"workload": f"{args.workload} n={n} depth={depth} seed={args.seed} "
                                    f"({n_gates} gates), fused ({prog.n_ops} device ops)",
                        "qubits": n, "depth": depth, "gates": n_gates,
                        "fusion_width": args.fusion_width or "default", "parallelism": f"replicas x{world}",
