@@ -96,6 +96,25 @@ def test_fused_trajectories_with_swaps(ref):
     assert got == want
 
 
+def test_fused_trajectories_with_pauli_rotations(ref):
+    """Pauli rotations of weight 2..8 between noisy layers run inside the register passes
+    (flips on register bits and lanes, Z qubits in and out of the tile) beside the per-state
+    noise matrices: counts equal the reference's per-shot semantics."""
+    rng = np.random.default_rng(31)
+    qc = lq.QuantumCircuit(12, 12)
+    qc.compose(W.brickwork(12, 2, seed=11, noise=(0.05, 0.1, 0.2)))
+    for _ in range(6):
+        w = int(rng.integers(2, 9))
+        q = [int(x) for x in rng.permutation(12)[:w]]
+        qc.rp(float(rng.uniform(-np.pi, np.pi)),
+              "".join("XYZ"[int(rng.integers(3))] for _ in range(w)), q)
+    qc.compose(W.brickwork(12, 2, seed=12, noise=(0.05, 0.1, 0.2)))
+    qc.measure_all()
+    want = counts_of(ref.trajectories(qc, 96, 23))
+    got = counts_of(lq.StatevectorSimulator(seed=23, max_resident=32).run_registers(qc, 96))
+    assert got == want
+
+
 def test_fused_noise_model_counts_identical(ref):
     noise = lq.NoiseModel()
     noise.add_all_qubit_channel(lq.KrausChannel.depolarizing(0.05))
