@@ -1,8 +1,8 @@
 """Parity at the headline sizes (28-30 qubits) and at the full shape of the batched
 gradient workload.
 
-* 30 qubits: the seeded brickwork of depth 40 (1800 gates) and QFT(30) on a random
-  Gaussian state, through the default path (register tile passes with searched high
+* 30 qubits: the seeded brickwork of depth 40 (1800 gates), QFT(30) and the cost-model gate
+  mix (Pauli rotations inside register passes) on a random Gaussian state, through the default path (register tile passes with searched high
   qubits), against the engine's own gate-by-gate path on a second 16 GiB state; compared on
   the device in chunks.
 * 26 to 30 qubits against the reference compiled from its own sources: the first two
@@ -95,6 +95,20 @@ def test_qft30_on_gaussian_state_tile_passes_equal_gate_by_gate():
     b.to_torch().copy_(a.to_torch())
     lq.simulator.CompiledCircuit(q, True, 0, 0).apply(a)
     lq.simulator.CompiledCircuit(q, True, 0, GATE_BY_GATE).apply(b)
+    assert _device_maxdiff(a, b) < TOL
+
+
+def test_random_mix_30q_native_rotations_equal_gate_by_gate():
+    """The cost-model gate mix at 30 qubits (Pauli rotations of weight 2..8 inside register
+    passes, their Z qubits in and out of the tile) from a Gaussian state, against gate-by-gate
+    application on a second 16 GiB state."""
+    qc = W.random_mix_circuit(30, 8, seed=31)
+    a = lq.Statevector(30)
+    _device_gaussian(a, seed=31)
+    b = lq.Statevector(30)
+    b.to_torch().copy_(a.to_torch())
+    lq.simulator.CompiledCircuit(qc, True, 0, 0).apply(a)
+    lq.simulator.CompiledCircuit(qc, True, 0, GATE_BY_GATE).apply(b)
     assert _device_maxdiff(a, b) < TOL
 
 
