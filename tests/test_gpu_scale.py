@@ -2,9 +2,9 @@
 gradient workload.
 
 * 30 qubits: the seeded brickwork of depth 40 (1800 gates), QFT(30) and the cost-model gate
-  mix (Pauli rotations inside register passes) on a random Gaussian state, through the default path (register tile passes with searched high
-  qubits), against the engine's own gate-by-gate path on a second 16 GiB state; compared on
-  the device in chunks.
+  mix (Pauli rotations inside register passes) on a random Gaussian state, through the
+  default path (register tile passes with searched high qubits), against the engine's own
+  gate-by-gate path on a second 16 GiB state; compared on the device in chunks.
 * 26 to 30 qubits against the reference compiled from its own sources: the first two
   brickwork layers of the headline circuit at 28 and 30 qubits (from |0..0>,
   `StatevectorSimulator::run_statevector`, src/backend/statevector_simulator.cpp:222-230)
