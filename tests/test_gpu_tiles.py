@@ -349,3 +349,50 @@ def test_random_mix_24q_native_rotations_equal_gate_by_gate():
     b = lq.Statevector.from_numpy(init)
     lq.simulator.CompiledCircuit(qc, True, 0, 3).apply(b)
     assert float(np.max(np.abs(a.to_numpy() - b.to_numpy()))) < TOL
+
+
+_SIGMA = {"I": np.eye(2), "X": np.array([[0, 1], [1, 0]], dtype=complex),
+          "Y": np.array([[0, -1j], [1j, 0]]), "Z": np.diag([1.0, -1.0]).astype(complex)}
+
+
+def _rotation_matrix(theta, pauli):
+    """exp(-i theta/2 P), matrix bit j <-> qubits[j], P's character pauli[k-1-j] on it."""
+    p = np.array([[1.0 + 0j]])
+    for ch in pauli:          # leftmost character = most significant matrix bit
+        p = np.kron(p, _SIGMA[ch])
+    return np.cos(theta / 2) * np.eye(p.shape[0]) - 1j * np.sin(theta / 2) * p
+
+
+def test_native_rotations_match_dense_matrices_and_named_gates():
+    """Known answers of the reference's Pauli-rotation tests (tests/test_pauli_rotation.cpp:
+    rp("XX"/"YY"/"ZZ") equal RXX/RYY/RZZ, the kernel equals the dense matrix for long
+    strings) at 16 qubits, where the rotations run inside register passes: each circuit of
+    rotations against the same circuit with the rotations as explicit unitaries or named
+    gates, from one Gaussian state, within 1e-12."""
+    n = 16
+    rng = np.random.default_rng(41)
+    init = W.gaussian_state(n, seed=41)
+    rot = lq.QuantumCircuit(n)
+    dense = lq.QuantumCircuit(n)
+    for _ in range(40):
+        w = int(rng.integers(1, 7))
+        qs = [int(x) for x in rng.permutation(n)[:w]]
+        pauli = "".join("XYZ"[int(rng.integers(3))] for _ in range(w))
+        th = float(rng.uniform(-np.pi, np.pi))
+        a = int(rng.integers(n))
+        rot.h(a).rp(th, pauli, qs)
+        dense.h(a).unitary(_rotation_matrix(th, pauli), qs)
+    got = run(rot, TILE, init)
+    assert 7 in kernel_kinds(rot)
+    assert np.max(np.abs(got - run(dense, GREEDY, init))) < TOL
+    named = lq.QuantumCircuit(n)
+    as_rp = lq.QuantumCircuit(n)
+    for i in range(30):
+        a, b = (int(x) for x in rng.permutation(n)[:2])
+        th = float(rng.uniform(-np.pi, np.pi))
+        kind = i % 3
+        named.h(a)
+        as_rp.h(a)
+        getattr(named, ("rxx", "ryy", "rzz")[kind])(th, a, b)
+        as_rp.rp(th, ("XX", "YY", "ZZ")[kind], [a, b])
+    assert np.max(np.abs(run(as_rp, TILE, init) - run(named, TILE, init))) < TOL
