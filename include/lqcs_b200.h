@@ -35,7 +35,8 @@ enum lqcs_status {
     LQCS_ERR_LOGIC = 3,
     LQCS_ERR_CUDA = 4,
     LQCS_ERR_OUT_OF_MEMORY = 5,
-    LQCS_ERR_TIMEOUT = 6,
+    LQCS_ERR_TIMEOUT = 6,   /* reserved: no entry point waits on a flag another rank or
+                               device sets, so none returns it */
     LQCS_ERR_INTERNAL = 7
 };
 
