@@ -264,7 +264,8 @@ struct AdjointPlan {
     std::vector<Segment> fwd_segs, bwd_segs;
     DeviceBuffer d_rot_ops, d_rot_part;
     cudaStream_t stream = nullptr;
-    std::map<uint32_t, std::pair<cudaGraphExec_t, uint64_t>> graphs;   // nb -> (graph, kernels)
+    // (2 nb + with gradients) -> (graph, kernels)
+    std::map<uint32_t, std::pair<cudaGraphExec_t, uint64_t>> graphs;
 
     AdjointPlan() = default;
     AdjointPlan(const AdjointPlan&) = delete;
@@ -301,8 +302,9 @@ struct AdjointPlan {
         }
     }
 
-    // The launch sequence of one batch of nb sets on this plan's stream.
-    void enqueue(uint32_t nb) const {
+    // The launch sequence of one batch of nb sets on this plan's stream; without gradients
+    // (energies only) it ends after <psi|H|psi>.
+    void enqueue(uint32_t nb, bool grads = true) const {
         const LaunchCtx& ctx = psi->ctx;
         const uint64_t len = uint64_t{1} << n;
         const RotTileOp* rot_ops = d_rot_ops.as<RotTileOp>();
@@ -324,6 +326,7 @@ struct AdjointPlan {
         }
         launch_batched_inner_re_p(ctx, psi->d(), lam->d(), n, nb, d_part.as<double>(),
                                   d_energy.as<double>());
+        if (!grads) return;
         if (bwd_segs.empty()) {
             for (size_t i = steps.size(); i-- > 0;) backward_step(steps[i], nb);
         } else {
@@ -388,13 +391,14 @@ struct AdjointPlan {
         d_rot_part.ensure(sizeof(double) * max_ops * R * (uint64_t{1} << (n - mb)));
     }
 
-    void run(uint32_t nb) {
+    void run(uint32_t nb, bool grads = true) {
         const char* e = std::getenv("LQCS_GRAPHS");
         if (e && e[0] == '0') {
-            enqueue(nb);
+            enqueue(nb, grads);
             return;
         }
-        auto it = graphs.find(nb);
+        const uint32_t key = 2 * nb + (grads ? 1u : 0u);
+        auto it = graphs.find(key);
         bool fresh = false;
         if (it == graphs.end()) {
             // capture once; a failed capture falls back to direct launches (which rethrow any
@@ -405,7 +409,7 @@ struct AdjointPlan {
             bool ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
             if (ok) {
                 try {
-                    enqueue(nb);
+                    enqueue(nb, grads);
                 } catch (...) {
                     ok = false;
                 }
@@ -418,10 +422,10 @@ struct AdjointPlan {
             if (g) cudaGraphDestroy(g);
             if (!ok) {
                 cudaGetLastError();
-                enqueue(nb);
+                enqueue(nb, grads);
                 return;
             }
-            it = graphs.emplace(nb, std::make_pair(exec, launch_count() - k0)).first;
+            it = graphs.emplace(key, std::make_pair(exec, launch_count() - k0)).first;
             fresh = true;   // the capture already counted this batch's kernels
         }
         cuda_check(cudaGraphLaunch(it->second.first, stream), "cudaGraphLaunch");
@@ -562,7 +566,7 @@ void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
             d_out.ensure(sizeof(double) * (np + 1));
             launch_batched_inner_re_p(st->ctx, st->d(), lam->d(), n, 1, part.as<double>(),
                                       d_out.as<double>() + np);
-            for (size_t i = tmpl.size(); i-- > 0;) {
+            for (size_t i = grad_out ? tmpl.size() : 0; i-- > 0;) {
                 const GateDesc& g = bound[i];
                 if (!g.is_unitary()) continue;
                 if (param_of[i] >= 0) {
@@ -605,10 +609,10 @@ void adjoint_batched(const lqcs_parametric_circuit* pc, const Hamiltonian& h,
             cuda_check(cudaMemcpyAsync(plan.d_csi.ptr, csi.data(), sizeof(double2) * np * R,
                                        cudaMemcpyHostToDevice, plan.stream), "H2D");
         }
-        plan.run(nb);
+        plan.run(nb, grad_out != nullptr);
         cuda_check(cudaMemcpyAsync(h_energy.data(), plan.d_energy.ptr, sizeof(double) * nb,
                                    cudaMemcpyDeviceToHost, plan.stream), "D2H energies");
-        if (np)
+        if (np && grad_out)
             cuda_check(cudaMemcpyAsync(h_grad.data(), plan.d_grad.ptr, sizeof(double) * np * nb,
                                        cudaMemcpyDeviceToHost, plan.stream), "D2H gradients");
         cuda_check(cudaStreamSynchronize(plan.stream), "adjoint");
