@@ -374,7 +374,8 @@ int lqcs_adjoint_gradient_multi(uint64_t n_problems, const lqcs_parametric_circu
  * the autotuner's choices.  Engine extension: no counterpart in the reference. */
 int lqcs_release_caches(void);
 
-/* Energies only, batched (forward pass of lqcs_adjoint_gradient). */
+/* Energies only, batched: the forward pass and <psi|H|psi> of lqcs_adjoint_gradient
+ * without its backward sweep (about half the time of the gradient call). */
 int lqcs_batched_energy(const lqcs_parametric_circuit* pc, const lqcs_hamiltonian* h,
                         const double* params, uint64_t batch, uint32_t max_resident,
                         double* energy_out);
