@@ -802,15 +802,16 @@ def run_extras(lq, W, N, n, sv, hbm_peak, args):
     if want("costmodel"):
         try:
             from litequantumcomputingsimulator_b200 import costmodel as CM
-            corpus = [(22 + (i % 5), 10 + (13 * i) % 51, 1000 + i) for i in range(24)]
+            # 25..27 qubits (0.5..2 GiB states): larger than L2, as the 32-qubit plans are
+            corpus = [(25 + (i % 3), 10 + (7 * i) % 21, 1000 + i) for i in range(12)]
             train_set = [W.random_mix_circuit(nq, d, s_) for nq, d, s_ in corpus]
             t0 = time.perf_counter()
             x, y = CM.collect(train_set)
             t1 = time.perf_counter()
             loss = CM.train(x, y, epochs=3000, lr=3e-3, seed=0)
             t_train = time.perf_counter() - t1
-            out["costmodel_corpus"] = {"circuits": len(corpus), "qubits": "22..26",
-                                       "depths": "10..60", "rows": int(y.size),
+            out["costmodel_corpus"] = {"circuits": len(corpus), "qubits": "25..27",
+                                       "depths": "10, 17, 24", "rows": int(y.size),
                                        "collect_s": t1 - t0}
             out["costmodel_train_rows_x_epochs_per_s"] = y.size * 3000 / t_train
             xi = np.repeat(x, max(1, 1_000_000 // max(1, len(x))), axis=0)
